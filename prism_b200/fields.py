@@ -1,0 +1,102 @@
+"""Seeded synthetic scientific fields used by the tests, the golden-fixture
+script and the benchmark.
+
+All fields are C-ordered numpy arrays ``a[z][y][x]`` (x fastest), i.e. the raw
+little-endian layout the PRISM CLI reads with ``-3 nx ny nz``.  The generators
+stand in for the datasets the reference's README names (SDRBench Miranda etc.),
+which are not available offline; they reproduce the shapes, dtypes and value
+distributions of the benchmark configurations.
+
+* ``sinusoid``   - sum of 8 random plane waves + N(0, 1e-3) noise (smooth).
+* ``grf``        - Gaussian random field with an isotropic k^-5/3 power
+                   spectrum (inverse rFFT of seeded complex normals), mapped
+                   affinely to [lo, hi].
+* ``voronoi``    - piecewise-smooth field: nearest-of-64-seeds cells, each a
+                   random quadratic polynomial, 30% of cells exactly 0.0, plus
+                   0.1% isolated spikes of +-1e3 (sparse/sharp).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def sinusoid(shape, dtype=np.float32, seed=0, waves=8, noise=1e-3):
+    """Sum of ``waves`` sinusoids with integer wavenumbers 1..8 per axis."""
+    nz, ny, nx = shape
+    rng = np.random.default_rng(seed)
+    amp = rng.uniform(0.1, 1.0, waves)
+    phase = rng.uniform(0.0, 2 * np.pi, waves)
+    k = rng.integers(1, 9, size=(waves, 3))
+    z = np.arange(nz, dtype=np.float64)[:, None, None] / max(nz, 1)
+    y = np.arange(ny, dtype=np.float64)[None, :, None] / max(ny, 1)
+    x = np.arange(nx, dtype=np.float64)[None, None, :] / max(nx, 1)
+    out = np.zeros(shape, dtype=np.float64)
+    for i in range(waves):
+        out += amp[i] * np.sin(2 * np.pi * (k[i, 0] * x + k[i, 1] * y + k[i, 2] * z) + phase[i])
+    out += rng.normal(0.0, noise, size=shape)
+    return out.astype(dtype)
+
+
+def grf(shape, dtype=np.float64, seed=1, slope=-5.0 / 3.0, lo=0.9, hi=3.0):
+    """Isotropic Gaussian random field with power spectrum P(k) ~ k^slope."""
+    rng = np.random.default_rng(seed)
+    nz, ny, nx = shape
+    kz = np.fft.fftfreq(nz)[:, None, None]
+    ky = np.fft.fftfreq(ny)[None, :, None]
+    kx = np.fft.rfftfreq(nx)[None, None, :]
+    kk = np.sqrt(kz * kz + ky * ky + kx * kx)
+    kk[0, 0, 0] = 1.0
+    amp = kk ** (slope / 2.0)
+    amp[0, 0, 0] = 0.0
+    spec = (rng.standard_normal(amp.shape) + 1j * rng.standard_normal(amp.shape)) * amp
+    f = np.fft.irfftn(spec, s=shape)
+    fmin, fmax = f.min(), f.max()
+    f = lo + (hi - lo) * (f - fmin) / (fmax - fmin)
+    return f.astype(dtype)
+
+
+def voronoi(shape, dtype=np.float32, seed=2, cells=64, zero_frac=0.3,
+            spike_frac=1e-3, spike_amp=1e3, slab=16):
+    """Piecewise-quadratic Voronoi field with zero cells and isolated spikes."""
+    rng = np.random.default_rng(seed)
+    nz, ny, nx = shape
+    seeds = rng.uniform(0.0, 1.0, size=(cells, 3)) * np.array([nz, ny, nx])
+    coef = rng.normal(0.0, 1.0, size=(cells, 10))
+    zero = rng.uniform(0.0, 1.0, cells) < zero_frac
+    coef[zero] = 0.0
+    out = np.empty(shape, dtype=dtype)
+    y = (np.arange(ny, dtype=np.float32) / ny)[None, :, None]
+    x = (np.arange(nx, dtype=np.float32) / nx)[None, None, :]
+    sy = np.arange(ny, dtype=np.float32)[None, :, None]
+    sx = np.arange(nx, dtype=np.float32)[None, None, :]
+    for z0 in range(0, nz, slab):
+        z1 = min(nz, z0 + slab)
+        sz = np.arange(z0, z1, dtype=np.float32)[:, None, None]
+        best = np.full((z1 - z0, ny, nx), np.inf, dtype=np.float32)
+        owner = np.zeros((z1 - z0, ny, nx), dtype=np.int16)
+        for c in range(cells):
+            d = (sz - seeds[c, 0]) ** 2 + (sy - seeds[c, 1]) ** 2 + (sx - seeds[c, 2]) ** 2
+            m = d < best
+            best = np.where(m, d, best)
+            owner = np.where(m, np.int16(c), owner)
+        zz = (sz / nz)
+        cc = coef[owner]
+        v = (cc[..., 0] + cc[..., 1] * x + cc[..., 2] * y + cc[..., 3] * zz
+             + cc[..., 4] * x * x + cc[..., 5] * y * y + cc[..., 6] * zz * zz
+             + cc[..., 7] * x * y + cc[..., 8] * y * zz + cc[..., 9] * x * zz)
+        out[z0:z1] = v.astype(dtype)
+    n = out.size
+    nspk = int(round(n * spike_frac))
+    if nspk:
+        idx = rng.choice(n, size=nspk, replace=False)
+        sign = np.where(rng.uniform(0.0, 1.0, nspk) < 0.5, -1.0, 1.0)
+        out.reshape(-1)[idx] = (sign * spike_amp).astype(dtype)
+    return out
+
+
+GENERATORS = {"sinusoid": sinusoid, "grf": grf, "voronoi": voronoi}
+
+
+def make(kind, shape, dtype, seed):
+    """Dispatch by generator name; ``shape`` is (nz, ny, nx)."""
+    return GENERATORS[kind](tuple(shape), dtype=np.dtype(dtype), seed=seed)
