@@ -1,0 +1,148 @@
+/*
+ * prism_b200 -- C ABI of the B200-native PRISM compression hot path.
+ *
+ * Drop-in boundary for PRISM's pipeline entry points.  Every call works on
+ * device pointers on a caller-supplied CUDA stream, returns a status code and
+ * never exits the process (the reference exits on CUDA errors, err.hpp:3-11).
+ * Containers are byte-compatible with the reference in both directions.
+ *
+ * Reference interfaces replaced (paths inside BingluCS/PRISM):
+ *   prism_compress              Compressor<T,i4>::init + compress_pipeline
+ *                               (include/compressor.hpp:44-52,
+ *                                src/compressor.cu:77-151) with REL range from
+ *                               StatBuffer::findMinMax (compressor.hpp:23-31)
+ *   prism_decompress            Compressor<T,i4>::decompress_pipeline
+ *                               (compressor.hpp:54-57, compressor.cu:153-164)
+ *   prism_progressive_open/step Compressor<T,i4>::decompress_progressive_pipeline
+ *                               (compressor.hpp:59-61, compressor.cu:166-190) with
+ *                               the begin/end/maxlevel state of prism_context
+ *                               (include/utils/parameters.hpp:54-55,
+ *                                src/loader/dataloader.cu:11)
+ *   stage entry points          spline_construct / spline_reconstruct /
+ *                               spline_progressive_reconstruct
+ *                               (include/predictor/InterpolationPredictor.hpp:12-21),
+ *                               convert_to_bitplane / inverse_convert_to_bitplane[_progressive]
+ *                               (include/predictor/bitplane.hpp:15-22),
+ *                               lossless_encode / lossless_decode[_progressive]
+ *                               (include/encoder/zbpc.hpp:11-15),
+ *                               findStrategy_h (include/loader/dataloader.hpp:8),
+ *                               extrema_scan (include/compressor.hpp:10)
+ *
+ * dtype_size: 4 = float (PRISM -f), 8 = double (-d).
+ * mode: 0 = ABS (-A), 1 = REL (-R).
+ * progressive: 0 = sign-magnitude planes (default CLI), 1 = negabinary (-prog).
+ * Dimensions: nx fastest (-3 nx ny nz; -2 nx ny; -1 nx).
+ */
+#ifndef PRISM_B200_H
+#define PRISM_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum prism_status {
+  PRISM_OK = 0,
+  PRISM_ERR_ARG = -1,        /* bad argument (dims, dtype, bound, capacity) */
+  PRISM_ERR_CUDA = -2,       /* CUDA runtime error */
+  PRISM_ERR_CORRUPT = -3,    /* container does not parse / decode */
+  PRISM_ERR_TIMEOUT = -4,    /* a device-side wait hit its iteration limit */
+  PRISM_ERR_NOMEM = -5       /* device workspace allocation failed */
+};
+
+typedef struct prism_handle prism_handle;
+typedef struct prism_prog prism_prog;
+
+/* Handle owning the device workspace (grown on demand, reused across calls). */
+int prism_create(prism_handle** out);
+void prism_destroy(prism_handle* h);
+/* Human-readable description of the last failure on this handle. */
+const char* prism_last_error(const prism_handle* h);
+
+/* Upper bound of the container size (all chunks stored raw). */
+uint64_t prism_max_container_size(uint32_t nx, uint32_t ny, uint32_t nz, int dtype_size);
+/* Size of the plane buffer (host aligned_size, io.cu:117-127) and the trailer. */
+uint64_t prism_plane_buffer_size(uint32_t nx, uint32_t ny, uint32_t nz);
+uint64_t prism_trailer_size(uint32_t nx, uint32_t ny, uint32_t nz, int dtype_size);
+
+/* Compress d_in (n values) into the container at d_out.  *out_size receives
+ * the container size.  flags_out (host, may be NULL) receives use_md[4] then
+ * reverse[4] as chosen by the auto-tuner. */
+int prism_compress(prism_handle* h, const void* d_in, int dtype_size, uint32_t nx, uint32_t ny,
+                   uint32_t nz, int mode, double bound, int progressive, void* d_out,
+                   uint64_t out_capacity, uint64_t* out_size, uint8_t flags_out[8], void* stream);
+
+/* Same, with host buffers: host->device copy of the input, compression, and
+ * device->host copy of the container all inside the call. */
+int prism_compress_host(prism_handle* h, const void* h_in, int dtype_size, uint32_t nx, uint32_t ny,
+                        uint32_t nz, int mode, double bound, int progressive, void* h_out,
+                        uint64_t out_capacity, uint64_t* out_size, void* stream);
+
+/* Full decompression of a non-progressive (sign-magnitude) container. */
+int prism_decompress(prism_handle* h, const void* d_container, uint64_t size, int dtype_size,
+                     uint32_t nx, uint32_t ny, uint32_t nz, int mode, double bound, void* d_out,
+                     void* stream);
+int prism_decompress_host(prism_handle* h, const void* h_container, uint64_t size, int dtype_size,
+                          uint32_t nx, uint32_t ny, uint32_t nz, int mode, double bound, void* h_out,
+                          void* stream);
+
+/* Progressive retrieval of a negabinary (-prog) container that stays resident
+ * on the device (the caller keeps d_container alive).  Each step picks the
+ * planes the target error needs, decodes only their chunks and refines the
+ * values in d_values in place (the first step overwrites them). */
+int prism_progressive_open(prism_handle* h, const void* d_container, uint64_t size, int dtype_size,
+                           uint32_t nx, uint32_t ny, uint32_t nz, int mode, double bound,
+                           prism_prog** out);
+int prism_progressive_step(prism_prog* p, double target_error, void* d_values, void* stream);
+/* begin/end/maxlevel after the last step; loaded = payload bytes of the
+ * planes selected so far (calculate_accumulate_size, analyze.hpp:118-159). */
+int prism_progressive_state(const prism_prog* p, int begin[4], int end[4], int* maxlevel,
+                            uint64_t* loaded);
+void prism_progressive_close(prism_prog* p);
+
+/* ---- stage entry points (device buffers; for tests and custom pipelines) */
+/* Global range max-min in double (extrema_scan). */
+int prism_extrema(prism_handle* h, const void* d_in, int dtype_size, uint64_t n, double* range_out,
+                  void* stream);
+/* Auto-tune error sums (15 values, host) and the decisions (use_md[4], reverse[4]). */
+int prism_autotune(prism_handle* h, const void* d_in, int dtype_size, uint32_t nx, uint32_t ny,
+                   uint32_t nz, double* errors_out, uint8_t flags_out[8], void* stream);
+/* Predictor + quantiser with given flags (use_md[4], reverse[4]); eb is the
+ * absolute bound, rel_eb selects the level schedule (0 for ABS).  Writes the
+ * level-major codes (prism_code_buffer_len entries) and the anchors. */
+uint64_t prism_code_buffer_len(uint32_t nx, uint32_t ny, uint32_t nz);
+int prism_predict(prism_handle* h, const void* d_in, int dtype_size, uint32_t nx, uint32_t ny,
+                  uint32_t nz, double eb, double rel_eb, const uint8_t flags[8], int32_t* d_codes,
+                  void* d_anchors, void* stream);
+/* Reconstruction from codes + anchors; d_old != NULL adds the previous values
+ * (progressive delta); maxlevel = 4 for a full reconstruction. */
+int prism_reconstruct(prism_handle* h, const int32_t* d_codes, const void* d_anchors, int dtype_size,
+                      uint32_t nx, uint32_t ny, uint32_t nz, double eb, double rel_eb,
+                      const uint8_t flags[8], int maxlevel, const void* d_old, void* d_out, void* stream);
+/* Codes -> planes (prism_plane_buffer_size bytes), including the bytes the
+ * reference leaves holding the predictor's scratch. */
+int prism_bitshuffle(prism_handle* h, const int32_t* d_codes, uint32_t nx, uint32_t ny, uint32_t nz,
+                     int progressive, uint8_t* d_planes, void* stream);
+/* Planes -> codes; begin/end (host, may be NULL) restrict each level to the
+ * planes [begin[3-l], end[3-l]) like the progressive inverse. */
+int prism_inverse_bitshuffle(prism_handle* h, const uint8_t* d_planes, uint32_t nx, uint32_t ny,
+                             uint32_t nz, int progressive, const int begin[4], const int end[4],
+                             int32_t* d_codes, void* stream);
+/* Planes -> lossless stream (8-byte header, size table, payloads, pad to 8);
+ * comp_size_bp (host, may be NULL) receives the 128 cumulative plane sizes. */
+int prism_lossless_encode(prism_handle* h, const uint8_t* d_planes, uint32_t nx, uint32_t ny,
+                          uint32_t nz, uint8_t* d_stream, uint64_t capacity, uint64_t* size_out,
+                          uint64_t comp_size_bp[128], void* stream);
+int prism_lossless_decode(prism_handle* h, const uint8_t* d_stream, uint32_t nx, uint32_t ny,
+                          uint32_t nz, const int begin[4], const int end[4], uint8_t* d_planes,
+                          void* stream);
+/* Strategy step: updates begin/end/maxlevel (host arrays) from the cumulative
+ * plane sizes (host), the absolute bound and the absolute target error. */
+int prism_find_strategy(prism_handle* h, const uint64_t comp_size_bp[128], double eb,
+                        double target_error, int begin[4], int end[4], int* maxlevel, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

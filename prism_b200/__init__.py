@@ -1,0 +1,231 @@
+"""prism_b200 -- B200-native PRISM compression hot path.
+
+Python side of the C ABI in ``include/prism_b200.h``.  Device memory is held in
+torch CUDA tensors (plumbing only); every computation runs in the sm_100a
+kernels of ``libprism_b200.so``.  There is no CPU fallback: importing works on
+any machine, but every call needs the library and a CUDA device and raises
+``PrismError`` otherwise.
+
+The names mirror the reference's ``prism::Compressor`` pipeline
+(include/compressor.hpp:35-83) and ``prism_context`` (include/utils/
+parameters.hpp:27-56): ``Context`` carries dims, dtype, error mode, bound and
+the SM/NB plane coding; ``Compressor`` offers ``compress_pipeline``,
+``decompress_pipeline`` and ``decompress_progressive_pipeline``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _build
+
+LIB_PATH = _build.LIB
+ABS, REL = 0, 1
+SM, NB = 0, 1  # progressive=0 -> sign-magnitude planes, 1 -> negabinary
+
+_STATUS = {0: "ok", -1: "bad argument", -2: "CUDA error", -3: "corrupt container",
+           -4: "device wait timed out", -5: "out of device memory"}
+
+
+class PrismError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def lib():
+    """Load libprism_b200.so (fails loudly if it is missing)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise PrismError(f"{LIB_PATH} is missing: run prism_b200._build.build_lib()")
+        l = C.CDLL(LIB_PATH)
+        vp, u32, u64, i32, dbl = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int, C.c_double
+        l.prism_create.argtypes = [C.POINTER(vp)]
+        l.prism_destroy.argtypes = [vp]
+        l.prism_last_error.argtypes = [vp]
+        l.prism_last_error.restype = C.c_char_p
+        for fn in ("prism_max_container_size", "prism_trailer_size"):
+            getattr(l, fn).argtypes = [u32, u32, u32, i32]
+            getattr(l, fn).restype = u64
+        for fn in ("prism_plane_buffer_size", "prism_code_buffer_len"):
+            getattr(l, fn).argtypes = [u32, u32, u32]
+            getattr(l, fn).restype = u64
+        l.prism_compress.argtypes = [vp, vp, i32, u32, u32, u32, i32, dbl, i32, vp, u64, C.POINTER(u64), vp, vp]
+        l.prism_compress_host.argtypes = [vp, vp, i32, u32, u32, u32, i32, dbl, i32, vp, u64, C.POINTER(u64), vp]
+        l.prism_decompress.argtypes = [vp, vp, u64, i32, u32, u32, u32, i32, dbl, vp, vp]
+        l.prism_decompress_host.argtypes = [vp, vp, u64, i32, u32, u32, u32, i32, dbl, vp, vp]
+        l.prism_progressive_open.argtypes = [vp, vp, u64, i32, u32, u32, u32, i32, dbl, C.POINTER(vp)]
+        l.prism_progressive_step.argtypes = [vp, dbl, vp, vp]
+        l.prism_progressive_state.argtypes = [vp, vp, vp, vp, vp]
+        l.prism_progressive_close.argtypes = [vp]
+        l.prism_extrema.argtypes = [vp, vp, i32, u64, C.POINTER(dbl), vp]
+        l.prism_autotune.argtypes = [vp, vp, i32, u32, u32, u32, vp, vp, vp]
+        l.prism_predict.argtypes = [vp, vp, i32, u32, u32, u32, dbl, dbl, vp, vp, vp, vp]
+        l.prism_reconstruct.argtypes = [vp, vp, vp, i32, u32, u32, u32, dbl, dbl, vp, i32, vp, vp, vp]
+        l.prism_bitshuffle.argtypes = [vp, vp, u32, u32, u32, i32, vp, vp]
+        l.prism_inverse_bitshuffle.argtypes = [vp, vp, u32, u32, u32, i32, vp, vp, vp, vp]
+        l.prism_lossless_encode.argtypes = [vp, vp, u32, u32, u32, vp, u64, C.POINTER(u64), vp, vp]
+        l.prism_lossless_decode.argtypes = [vp, vp, u32, u32, u32, vp, vp, vp, vp]
+        l.prism_find_strategy.argtypes = [vp, vp, dbl, dbl, vp, vp, vp, vp]
+        _lib = l
+    return _lib
+
+
+EXPORTED = [
+    "prism_create", "prism_destroy", "prism_last_error", "prism_max_container_size",
+    "prism_plane_buffer_size", "prism_trailer_size", "prism_compress", "prism_compress_host",
+    "prism_decompress", "prism_decompress_host", "prism_progressive_open", "prism_progressive_step",
+    "prism_progressive_state", "prism_progressive_close", "prism_extrema", "prism_autotune",
+    "prism_code_buffer_len", "prism_predict", "prism_reconstruct", "prism_bitshuffle",
+    "prism_inverse_bitshuffle", "prism_lossless_encode", "prism_lossless_decode", "prism_find_strategy",
+]
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise PrismError("prism_b200 needs a CUDA device")
+    return torch
+
+
+class Handle:
+    """Owns a prism_handle (device workspace cache)."""
+
+    def __init__(self):
+        self.ptr = C.c_void_p()
+        rc = lib().prism_create(C.byref(self.ptr))
+        if rc:
+            raise PrismError(f"prism_create failed ({_STATUS.get(rc, rc)})")
+
+    def check(self, rc, what):
+        if rc:
+            msg = lib().prism_last_error(self.ptr)
+            raise PrismError(f"{what}: {_STATUS.get(rc, rc)}: {msg.decode() if msg else ''}")
+
+    def close(self):
+        if self.ptr:
+            lib().prism_destroy(self.ptr)
+            self.ptr = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _stream(torch):
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+@dataclass
+class Context:
+    """The fields of the reference's prism_context that the path uses."""
+    nx: int
+    ny: int = 1
+    nz: int = 1
+    dtype: np.dtype = np.dtype(np.float32)
+    error_mode: int = REL
+    bound: float = 1e-4          # -R rel_eb or -A eb
+    progressive: bool = False    # -prog (negabinary planes)
+    targets: list = field(default_factory=list)  # -errors
+
+    @property
+    def tsize(self):
+        return np.dtype(self.dtype).itemsize
+
+    @property
+    def shape(self):
+        return (self.nz, self.ny, self.nx)
+
+
+class Compressor:
+    """Device-side compress / decompress / progressive retrieval of one field."""
+
+    def __init__(self, ctx: Context, handle: Handle | None = None):
+        self.ctx = ctx
+        self.h = handle or Handle()
+        self.flags = None
+
+    def max_container_size(self):
+        c = self.ctx
+        return int(lib().prism_max_container_size(c.nx, c.ny, c.nz, c.tsize))
+
+    def compress_pipeline(self, d_in, d_out=None):
+        """d_in: CUDA tensor of the field; returns a uint8 CUDA tensor (container)."""
+        torch = _torch()
+        c = self.ctx
+        cap = self.max_container_size()
+        if d_out is None:
+            d_out = torch.empty(cap, dtype=torch.uint8, device=d_in.device)
+        size = C.c_uint64(0)
+        flags = (C.c_uint8 * 8)()
+        rc = lib().prism_compress(self.h.ptr, C.c_void_p(d_in.data_ptr()), c.tsize, c.nx, c.ny, c.nz,
+                                  c.error_mode, c.bound, int(c.progressive), C.c_void_p(d_out.data_ptr()),
+                                  d_out.numel(), C.byref(size), flags, _stream(torch))
+        self.h.check(rc, "prism_compress")
+        self.flags = (tuple(flags[:4]), tuple(flags[4:]))
+        return d_out[: size.value]
+
+    def decompress_pipeline(self, d_cont, d_out=None):
+        torch = _torch()
+        c = self.ctx
+        if d_out is None:
+            d_out = torch.empty(c.shape, dtype=_torch_dtype(torch, c.dtype), device=d_cont.device)
+        rc = lib().prism_decompress(self.h.ptr, C.c_void_p(d_cont.data_ptr()), d_cont.numel(), c.tsize, c.nx,
+                                    c.ny, c.nz, c.error_mode, c.bound, C.c_void_p(d_out.data_ptr()),
+                                    _stream(torch))
+        self.h.check(rc, "prism_decompress")
+        return d_out
+
+    def progressive(self, d_cont):
+        return Progressive(self, d_cont)
+
+
+class Progressive:
+    """decompress_progressive_pipeline as a resident object: each step refines
+    the reconstruction in place (compressor.cu:166-190)."""
+
+    def __init__(self, comp: Compressor, d_cont):
+        torch = _torch()
+        self.comp = comp
+        self.cont = d_cont
+        c = comp.ctx
+        self.ptr = C.c_void_p()
+        rc = lib().prism_progressive_open(comp.h.ptr, C.c_void_p(d_cont.data_ptr()), d_cont.numel(), c.tsize, c.nx,
+                                          c.ny, c.nz, c.error_mode, c.bound, C.byref(self.ptr))
+        comp.h.check(rc, "prism_progressive_open")
+        self.values = torch.zeros(c.shape, dtype=_torch_dtype(torch, c.dtype), device=d_cont.device)
+
+    def step(self, target):
+        torch = _torch()
+        rc = lib().prism_progressive_step(self.ptr, target, C.c_void_p(self.values.data_ptr()), _stream(torch))
+        self.comp.h.check(rc, "prism_progressive_step")
+        return self.values
+
+    def state(self):
+        b = (C.c_int * 4)()
+        e = (C.c_int * 4)()
+        ml = C.c_int()
+        lib().prism_progressive_state(self.ptr, b, e, C.byref(ml), None)
+        return list(b), list(e), ml.value
+
+    def close(self):
+        if self.ptr:
+            lib().prism_progressive_close(self.ptr)
+            self.ptr = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _torch_dtype(torch, dt):
+    return torch.float32 if np.dtype(dt) == np.float32 else torch.float64

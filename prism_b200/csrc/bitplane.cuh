@@ -163,27 +163,156 @@ inverse_bitshuffle_kernel(const uint8_t* __restrict__ planes, int32_t* __restric
   }
 }
 
-// Zero bytes the reference's last shuffle block writes past the processed
-// codes (bitplane.cu:243-259: whole 512-code rounds, `write_pos < res`).
-// Launched after bitshuffle_kernel so these writes land last, as in the
-// reference where that block runs last.  One thread per group of 8 codes.
-__global__ void shuffle_zero_tail_kernel(uint8_t* __restrict__ planes, Geometry g, int64_t zfirst,
-                                         int64_t zend, uint64_t limit) {
-  int64_t grp = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  int64_t c = zfirst + grp * 8;
-  if (c >= zend) return;
+// ---- the reference's last shuffle block, reproduced thread by thread ----
+//
+// In bitplane.cu the element count of the last block is res = align + tail,
+// but `align` is a local that d_comput only updates in thread 0
+// (bitplane.cu:32-57, 90-91), so thread 0 uses align + tail and every other
+// thread uses tail (= n % 16384, or 16384).  The block iterates in rounds of
+// 512 codes; a round's writer t stores the transposed word of position
+// 8*(t&63) + (t>>6) when that index (not the position) is below its own res
+// (`write_pos < res`, :246), which writes zero words past the data and skips
+// some real ones.  Lanes outside the active set read 0 from their partners in
+// the 8-lane network (their register holds the 0 they were initialised with).
+// These kernels run that logic with one CTA of 512 threads and an explicit
+// shared-memory emulation of the shuffle network, so the outcome is fixed.
+
+__device__ __forceinline__ uint32_t bperm(uint32_t x, uint32_t y, uint32_t s) { return __byte_perm(x, y, s); }
+
+// one xor-shuffle/byte_perm step of the 8-lane network (bitplane.cu:112-124)
+__device__ __forceinline__ uint32_t net_step(uint32_t a, uint32_t q, int lane8, int step) {
+  if (step == 0) return (lane8 & 4) == 0 ? bperm(a, q, 0x3276) : bperm(a, q, 0x5410);
+  if (step == 1) return (lane8 & 2) == 0 ? bperm(a, q, 0x3715) : bperm(a, q, 0x6240);
+  const uint32_t mask = 0x0F0F0F0Fu;
+  return (lane8 & 1) == 0 ? ((a & ~mask) | ((q >> 4) & mask)) : (((q << 4) & ~mask) | (a & mask));
+}
+__device__ __forceinline__ uint32_t bits_fwd(uint32_t a) {
+  uint32_t q;
+  q = (a ^ (a >> 3)) & 0x0A0A0A0AU; a = a ^ q ^ (q << 3);
+  q = (a ^ (a >> 6)) & 0x00CC00CCU; a = a ^ q ^ (q << 6);
+  q = (a ^ (a >> 12)) & 0x0000F0F0U; a = a ^ q ^ (q << 12);
+  return a;
+}
+__device__ __forceinline__ uint32_t bits_inv(uint32_t a) {
+  uint32_t q;
+  q = (a ^ (a >> 12)) & 0x0000F0F0U; a = a ^ q ^ (q << 12);
+  q = (a ^ (a >> 6)) & 0x00CC00CCU; a = a ^ q ^ (q << 6);
+  q = (a ^ (a >> 3)) & 0x0A0A0A0AU; a = a ^ q ^ (q << 3);
+  return a;
+}
+
+__device__ __forceinline__ int64_t last_res_of(const Geometry& g, int t) {
+  int64_t tail = (int64_t)(g.n % kChunk);
+  if (tail == 0) tail = kChunk;
+  return tail + (t == 0 ? g.align_dev : 0);
+}
+
+// device position -> byte of plane 4*(c&7) (bitplane.cu:143-149)
+__device__ __forceinline__ int64_t place_dev(const Geometry& g, int64_t c, int64_t* stride) {
   int level = 0;
   while (level < 3 && c < g.dprefix[level]) ++level;
-  int64_t gbyte = (c - g.dprefix[level]) >> 3;
-  for (int p = 0; p < 32; ++p) {
-    uint64_t s = (uint64_t)(gbyte + g.dstride[level] * p + g.daprefix[level]);
-    if (s < limit) planes[s] = 0;
+  int64_t idx = c - g.dprefix[level];
+  *stride = g.dstride[level];
+  return (idx >> 3) + g.dstride[level] * ((idx & 7) << 2) + g.daprefix[level];
+}
+
+__global__ void __launch_bounds__(512)
+shuffle_last_block_kernel(const int32_t* __restrict__ codes, uint8_t* __restrict__ planes, Geometry g,
+                          int nb, uint64_t limit) {
+  __shared__ uint32_t a[512];
+  __shared__ uint32_t shm[512];
+  __shared__ unsigned char act[512];
+  const int t = threadIdx.x;
+  const int64_t start = (g.sh_grid - 1) * (int64_t)kChunk;
+  const int64_t res = last_res_of(g, t);
+  const int64_t ares = (res + 511) / 512 * 512;
+  const int64_t maxa = (last_res_of(g, 0) + 511) / 512 * 512;
+  shm[t] = 0;
+  for (int64_t base = 0; base < maxa; base += 512) {
+    bool part = base < ares;
+    bool ac = part && base + t < res;
+    act[t] = ac;
+    a[t] = ac ? sign_transform(codes[start + base + t], nb) : 0u;
+    __syncthreads();
+    for (int step = 0; step < 3; ++step) {
+      int partner = t ^ (4 >> step);
+      uint32_t q = act[partner] ? a[partner] : 0u;
+      uint32_t v = ac ? net_step(a[t], q, t & 7, step) : 0u;
+      __syncthreads();
+      a[t] = v;
+      __syncthreads();
+    }
+    if (part) shm[t] = ac ? bits_fwd(a[t]) : 0u;
+    __syncthreads();
+    int wp = ((t & 63) << 3) + (t >> 6);
+    if (part && wp < res) {
+      uint32_t w = shm[wp];
+      int64_t st;
+      int64_t s = place_dev(g, start + base + wp, &st);
+      uint8_t b[4] = {(uint8_t)(w >> 24), (uint8_t)(w >> 8), (uint8_t)(w >> 16), (uint8_t)w};
+      for (int j = 0; j < 4; ++j) {
+        uint64_t o = (uint64_t)(s + j * st);
+        if (o < limit) planes[o] = b[j];
+      }
+    }
+    __syncthreads();
   }
 }
 
-// Bytes the reference's shuffle never writes keep the predictor's linear
-// int32 scratch (it reuses the plane buffer, compressor.cu:328): byte b is
-// byte b%4 of the code of grid point b/4 (0 for anchors and b/4 >= n).
+// inverse of the last block (bitplane.cu:400-450 and :532-600): thread t
+// decodes positions t, t+512, ... below its own res; lanes that left the loop
+// supply 0 to the network.  begin/end (device, may be null) mask planes.
+__global__ void __launch_bounds__(512)
+inverse_last_block_kernel(const uint8_t* __restrict__ planes, int32_t* __restrict__ codes, Geometry g, int nb,
+                          const int* __restrict__ begin, const int* __restrict__ end, uint64_t limit) {
+  __shared__ uint32_t a[512];
+  __shared__ unsigned char act[512];
+  const int t = threadIdx.x;
+  const int64_t start = (g.sh_grid - 1) * (int64_t)kChunk;
+  const int64_t res = last_res_of(g, t);
+  const int64_t maxr = last_res_of(g, 0);
+  for (int64_t base = 0; base < maxr; base += 512) {
+    int64_t c = start + base + t;
+    bool ac = base + t < res;
+    uint32_t v = 0;
+    if (ac) {
+      int level = 0;
+      while (level < 3 && c < g.dprefix[level]) ++level;
+      int64_t st;
+      int64_t s = place_dev(g, c, &st);
+      int lane = (int)(((c - g.dprefix[level]) & 7) << 2);
+      int lo = 0, hi = 32;
+      if (begin) { lo = begin[3 - level]; hi = end[3 - level]; }
+      if (lo < hi) {
+        const int sh[4] = {24, 8, 16, 0};
+        for (int j = 0; j < 4; ++j) {
+          uint64_t o = (uint64_t)(s + j * st);
+          if (lane + j >= lo && lane + j < hi && o < limit) v |= (uint32_t)planes[o] << sh[j];
+        }
+      }
+      v = bits_inv(v);
+    }
+    act[t] = ac;
+    a[t] = v;
+    __syncthreads();
+    for (int step = 0; step < 3; ++step) {
+      int partner = t ^ (4 >> step);
+      uint32_t q = act[partner] ? a[partner] : 0u;
+      uint32_t nv = ac ? net_step(a[t], q, t & 7, step) : 0u;
+      __syncthreads();
+      a[t] = nv;
+      __syncthreads();
+    }
+    if (ac) codes[c] = sign_inverse(a[t], nb);
+    __syncthreads();
+  }
+}
+
+// The plane buffer starts out holding the predictor's linear int32 codes (the
+// reference reuses that buffer, compressor.cu:328); bytes the shuffle never
+// overwrites keep them.  Byte b holds byte b%4 of the code of grid point b/4
+// (0 for anchors and past n).  This fills the ranges the bulk shuffle does not
+// write; the last-block kernel then overwrites what it writes.
 struct ByteRange { uint64_t start, len; };
 
 __global__ void leftover_fill_kernel(uint8_t* __restrict__ planes, const int32_t* __restrict__ qc, Geometry g,
@@ -206,37 +335,35 @@ __global__ void leftover_fill_kernel(uint8_t* __restrict__ planes, const int32_t
   }
 }
 
-// The byte ranges of [0, aligned_size) that the reference shuffle leaves
-// untouched (per-plane slack, codes it never processes, the tail past the
-// device placement), excluding the zero-tail bytes.
-inline int leftover_ranges(const Geometry& g, const ShuffleSpan& sp, ByteRange* out, int cap) {
+// Byte ranges of the plane buffer the bulk shuffle (positions before the
+// last block) does not write: per plane, from the first group the bulk kernel
+// leaves to the stride end, and the tail past the device placement.
+inline int fill_ranges(const Geometry& g, const ShufPlan& plan, ByteRange* out, int cap) {
   int cnt = 0;
-  auto push = [&](int64_t a, int64_t b) {
-    if (b > a && cnt < cap) out[cnt++] = ByteRange{(uint64_t)a, (uint64_t)(b - a)};
-  };
-  int64_t lim_real = sp.processed < sp.end0 ? sp.processed : sp.end0;
-  int64_t seg_end[4] = {sp.end0, g.dprefix[0], g.dprefix[1], g.dprefix[2]};
-  int64_t seg_start[4] = {g.dprefix[0], g.dprefix[1], g.dprefix[2], 0};
-  int64_t z0 = lim_real, z1 = sp.written_end > lim_real ? sp.written_end : lim_real;  // zero tail
   for (int l = 3; l >= 0; --l) {
-    int64_t e = seg_end[l] < lim_real ? seg_end[l] : lim_real;
-    int64_t groups = e > seg_start[l] ? (e - seg_start[l]) / 8 : 0;
-    int64_t from = groups;
-    if (l == 0 && z1 > z0) from = (z1 - seg_start[0]) / 8;  // zero tail covers [groups, zg1)
-    for (int p = 0; p < 32; ++p) {
+    int64_t from = plan.proc[l] / 8;
+    if (from >= g.dstride[l]) continue;
+    for (int p = 0; p < 32 && cnt < cap; ++p) {
       int64_t base = g.daprefix[l] + (int64_t)p * g.dstride[l];
-      push(base + from, base + g.dstride[l]);
+      out[cnt++] = ByteRange{(uint64_t)(base + from), (uint64_t)(g.dstride[l] - from)};
     }
   }
-  int64_t tail_a = g.dev_total, tail_b = (int64_t)g.aligned_size;
-  if (z1 > z0) {  // plane 31 of level 0 may spill zeros past the device placement
-    int64_t zs = g.daprefix[0] + 31 * g.dstride[0] + (z0 - seg_start[0]) / 8;
-    int64_t ze = g.daprefix[0] + 31 * g.dstride[0] + (z1 - seg_start[0]) / 8;
-    if (zs < tail_a) zs = tail_a;
-    if (ze > zs) { push(tail_a, zs < tail_b ? zs : tail_b); tail_a = ze; }
-  }
-  push(tail_a, tail_b);
+  if ((uint64_t)g.dev_total < g.aligned_size && cnt < cap)
+    out[cnt++] = ByteRange{(uint64_t)g.dev_total, g.aligned_size - (uint64_t)g.dev_total};
   return cnt;
+}
+
+// Whether the reference's last block writes after the others where they
+// overlap (see the oracle): with more blocks than a B200 holds at once
+// (148 SMs x 4 CTAs of 512 threads) it starts after the first wave finished;
+// otherwise the loop round of each side decides.
+inline bool last_block_lands_last(const Geometry& g) {
+  if (g.sh_grid > 148 * 4) return true;
+  int64_t tail = (int64_t)(g.n % kChunk);
+  if (tail == 0) tail = kChunk;
+  int64_t it_last = (tail + 511) / 512 - 1;
+  int64_t it_first = (g.dprefix[0] % kChunk) / 512;
+  return it_first <= it_last;
 }
 
 }  // namespace prism_b200

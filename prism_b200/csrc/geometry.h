@@ -35,6 +35,7 @@ struct Geometry {
   uint64_t n;
   uint32_t ax, ay, az;  // anchor grid
   uint64_t anchors;
+  uint64_t grid[4];      // points of the stride-2, 4, 8, 16 grids
   // level-major order
   uint64_t leaps[5][2];  // grid extent in x and x*y at each level
   uint64_t lm_prefix[5]; // first level-major slot of each level (incl. anchors)
@@ -87,6 +88,7 @@ inline void make_geometry(uint32_t nx, uint32_t ny, uint32_t nz, int tsize, Geom
       grid[level] = sx * sy * sz;  // points of the stride-2^(level+1) grid
     }
   }
+  for (int l = 0; l < 4; ++l) g->grid[l] = grid[l];
   // level-major slots: pad levels 3..1 to x8
   for (int l = 0; l < 4; ++l) g->lm_prefix[l] = grid[l];
   g->lm_prefix[4] = 0;
@@ -161,27 +163,6 @@ PRISM_HD uint64_t level_major_index(const Geometry& g, uint64_t gx, uint64_t gy,
            (uint64_t)(((gz | gy) & 1) == 0) * ((gx + 1) >> 1);
   }
   return gid;
-}
-
-// Shuffle bookkeeping of the reference (bitplane.cu:98-260):
-//  processed = code positions whose planes receive real data;
-//  written_end = positions whose (possibly zero) bytes are written;
-//  end0 = end of the device level-0 segment.
-struct ShuffleSpan {
-  int64_t processed;
-  int64_t written_end;
-  int64_t end0;
-};
-
-PRISM_HD ShuffleSpan shuffle_span(const Geometry& g) {
-  ShuffleSpan s;
-  int64_t start = (g.sh_grid - 1) * (int64_t)kChunk;
-  int64_t res = g.sh_res;
-  int64_t align_res = (res + 511) / 512 * 512;
-  s.processed = start + res;
-  s.written_end = start + (res >= 512 ? align_res : res);
-  s.end0 = (int64_t)g.n + g.align_dev;
-  return s;
 }
 
 }  // namespace prism_b200

@@ -71,6 +71,13 @@ struct Expr {
     s = F::sub(s, t3);
     return F::mul(s, T(0.125));
   }
+  // the same expression inside the md cube stage is contracted the other way
+  // round: fma(6, t2, 3*t1) - t3 (measured against the reference build)
+  static __device__ __forceinline__ T quad_r_cube(T t1, T t2, T t3) {
+    T s = F::fma(T(6), t2, F::mul(T(3), t1));
+    s = F::sub(s, t3);
+    return F::mul(s, T(0.125));
+  }
   static __device__ __forceinline__ T lin(T a, T b) { return F::mul(F::add(a, b), T(0.5)); }
   static __device__ __forceinline__ T half(T a) { return F::mul(a, T(0.5)); }
 };
@@ -81,24 +88,24 @@ constexpr int kWinVol = kWin * kWin * kWin;
 template <class T>
 struct TileCtx {
   T* s;  // shared window, s[(z*17 + y)*17 + x]
-  uint32_t bi[3], gd[3];
+  uint32_t gs[3];      // global start of the window (uint32 arithmetic)
+  bool notlast[3];     // the window does not reach the field's end
   uint32_t dim[3];
   __device__ __forceinline__ T& at(int x, int y, int z) const { return s[(z * kWin + y) * kWin + x]; }
   __device__ __forceinline__ T get(int axis, int x, int y, int z, int c) const {
     return axis == 0 ? at(c, y, z) : (axis == 1 ? at(x, c, z) : at(x, y, c));
   }
   __device__ __forceinline__ bool in_data(int x, int y, int z) const {
-    return bi[0] * 16u + x < dim[0] && bi[1] * 16u + y < dim[1] && bi[2] * 16u + z < dim[2];
+    return gs[0] + (uint32_t)x < dim[0] && gs[1] + (uint32_t)y < dim[1] && gs[2] + (uint32_t)z < dim[2];
   }
   // xyz_predicate (:1173-1185); the exclusive form is used by the last stage
   // of level 0
   __device__ __forceinline__ bool pred_ok(int x, int y, int z, bool inclusive) const {
     if (inclusive) return in_data(x, y, z);
-    return x < 16 && y < 16 && z < 16 + (bi[2] == gd[2] - 1) && in_data(x, y, z);
+    return x < 16 && y < 16 && z < 16 + !notlast[2] && in_data(x, y, z);
   }
   __device__ __forceinline__ bool owned(int x, int y, int z) const {
-    return (x < 16 || bi[0] == gd[0] - 1) && (y < 16 || bi[1] == gd[1] - 1) &&
-           (z < 16 || bi[2] == gd[2] - 1);
+    return (x < 16 || !notlast[0]) && (y < 16 || !notlast[1]) && (z < 16 || !notlast[2]);
   }
 };
 
@@ -117,8 +124,8 @@ __device__ __forceinline__ T pred_line(const TileCtx<T>& t, int axis, int x, int
                                        bool md, bool nat) {
   using E = Expr<T>;
   int ix = axis == 0 ? x : (axis == 1 ? y : z);
-  uint32_t gx = t.bi[axis] * 16u + ix, gs = t.dim[axis];
-  bool c1 = t.bi[axis] != t.gd[axis] - 1;
+  uint32_t gx = t.gs[axis] + (uint32_t)ix, gs = t.dim[axis];
+  bool c1 = t.notlast[axis];
   bool c2 = ix >= 3 * u, c3 = ix + 3 * u <= 16;
   bool c4 = gx + 3u * u < gs, c5 = gx + (uint32_t)u < gs;
   T t1 = t.get(axis, x, y, z, nb_idx(ix, u, 1));
@@ -139,8 +146,8 @@ __device__ __forceinline__ T pred_line(const TileCtx<T>& t, int axis, int x, int
 // get_interp_order (:1538-1545): 4 cubic, 3 quad-left, 2 quad-right, 1 linear, 0 none
 template <class T>
 __device__ __forceinline__ int interp_order(const TileCtx<T>& t, int axis, int c, int u) {
-  uint32_t gx = t.bi[axis] * 16u + c, gs = t.dim[axis];
-  bool notlast = t.bi[axis] != t.gd[axis] - 1;
+  uint32_t gx = t.gs[axis] + (uint32_t)c, gs = t.dim[axis];
+  bool notlast = t.notlast[axis];
   int b = c >= 3 * u ? 3 : 1;
   int f = (c + 3 * u <= 16 && (notlast || gx + 3u * u < gs)) ? 3 : ((notlast || gx + (uint32_t)u < gs) ? 1 : 0);
   return b == 3 ? (f == 3 ? 4 : (f == 1 ? 3 : 0)) : (f == 3 ? 2 : (f == 1 ? 1 : 0));
@@ -205,7 +212,7 @@ __device__ __forceinline__ T pred_cube(const TileCtx<T>& t, int x, int y, int z,
   if (oy == 4) return cy();
   if (ox == 4) return cx();
   if (ox == 3) return E::quad_l(tx[0], tx[1], tx[2]);
-  if (ox == 2) return E::quad_r(tx[1], tx[2], tx[3]);
+  if (ox == 2) return E::quad_r_cube(tx[1], tx[2], tx[3]);
   if (ox == 1) return E::lin(tx[1], tx[2]);
   return tx[1];
 }
@@ -230,7 +237,7 @@ struct StageRunner {
   int32_t* qc;
   T ebr, ebx2;
   __device__ __forceinline__ void emit(int x, int y, int z, T pred) const {
-    uint64_t gx = t.bi[0] * 16ull + x, gy = t.bi[1] * 16ull + y, gz = t.bi[2] * 16ull + z;
+    uint64_t gx = (uint64_t)t.gs[0] + x, gy = (uint64_t)t.gs[1] + y, gz = (uint64_t)t.gs[2] + z;
     if (COMPRESS) {
       T rec;
       int32_t code = quantize(t.at(x, y, z), pred, ebr, ebx2, &rec);
@@ -329,20 +336,22 @@ predict_compress_kernel(const T* __restrict__ data, Geometry g, const PredParams
   uint32_t tile = blockIdx.x;
   TileCtx<T> t;
   t.s = win;
-  t.gd[0] = g.ax; t.gd[1] = g.ay; t.gd[2] = g.az;
-  t.bi[0] = tile % g.ax; t.bi[1] = (tile / g.ax) % g.ay; t.bi[2] = tile / g.ax / g.ay;
+  uint32_t bi[3] = {tile % g.ax, (tile / g.ax) % g.ay, tile / g.ax / g.ay};
+  uint32_t gd[3] = {g.ax, g.ay, g.az};
   t.dim[0] = g.nx; t.dim[1] = g.ny; t.dim[2] = g.nz;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) { t.gs[d] = bi[d] * 16u; t.notlast[d] = bi[d] != gd[d] - 1; }
   if (threadIdx.x == 0) p = *pp;
   const uint64_t sy = g.nx, sz = (uint64_t)g.nx * g.ny;
   for (int i = threadIdx.x; i < kWinVol; i += blockDim.x) {
     int x = i % kWin, y = (i / kWin) % kWin, z = i / (kWin * kWin);
     T v = T(0);
     if (t.in_data(x, y, z))
-      v = data[(t.bi[0] * 16ull + x) + (t.bi[1] * 16ull + y) * sy + (t.bi[2] * 16ull + z) * sz];
+      v = data[((uint64_t)t.gs[0] + x) + ((uint64_t)t.gs[1] + y) * sy + ((uint64_t)t.gs[2] + z) * sz];
     win[i] = v;
   }
   __syncthreads();
-  if (threadIdx.x == 0) anchors[t.bi[0] + (uint64_t)t.bi[1] * g.ax + (uint64_t)t.bi[2] * g.ax * g.ay] = win[0];
+  if (threadIdx.x == 0) anchors[bi[0] + (uint64_t)bi[1] * g.ax + (uint64_t)bi[2] * g.ax * g.ay] = win[0];
   run_levels<T, true>(t, g, p, qc);
 }
 
@@ -357,26 +366,28 @@ reconstruct_kernel(const int32_t* __restrict__ qc, const T* __restrict__ anchors
   uint32_t tile = blockIdx.x;
   TileCtx<T> t;
   t.s = win;
-  t.gd[0] = g.ax; t.gd[1] = g.ay; t.gd[2] = g.az;
-  t.bi[0] = tile % g.ax; t.bi[1] = (tile / g.ax) % g.ay; t.bi[2] = tile / g.ax / g.ay;
+  uint32_t bi[3] = {tile % g.ax, (tile / g.ax) % g.ay, tile / g.ax / g.ay};
+  uint32_t gd[3] = {g.ax, g.ay, g.az};
   t.dim[0] = g.nx; t.dim[1] = g.ny; t.dim[2] = g.nz;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) { t.gs[d] = bi[d] * 16u; t.notlast[d] = bi[d] != gd[d] - 1; }
   if (threadIdx.x == 0) p = *pp;
   for (int i = threadIdx.x; i < kWinVol; i += blockDim.x) win[i] = T(0);
   __syncthreads();
   if (threadIdx.x < 8) {  // x_reset_scratch_data (:1027-1067): anchors at the corners
     int x = (threadIdx.x & 1) * 16, y = ((threadIdx.x >> 1) & 1) * 16, z = (threadIdx.x >> 2) * 16;
-    uint32_t ax = x / 16 + t.bi[0], ay = y / 16 + t.bi[1], az = z / 16 + t.bi[2];
+    uint32_t ax = x / 16 + bi[0], ay = y / 16 + bi[1], az = z / 16 + bi[2];
     if (ax < g.ax && ay < g.ay && az < g.az) win[(z * kWin + y) * kWin + x] = anchors[ax + (uint64_t)ay * g.ax + (uint64_t)az * g.ax * g.ay];
   }
   __syncthreads();
   run_levels<T, false>(t, g, p, const_cast<int32_t*>(qc));
   const uint64_t sy = g.nx, sz = (uint64_t)g.nx * g.ny;
-  int xs = 16 + (t.bi[0] == g.ax - 1), ys = 16 + (t.bi[1] == g.ay - 1), zs = 16 + (t.bi[2] == g.az - 1);
+  int xs = 16 + !t.notlast[0], ys = 16 + !t.notlast[1], zs = 16 + !t.notlast[2];
   int total = xs * ys * zs;
   for (int i = threadIdx.x; i < total; i += blockDim.x) {
     int x = i % xs, y = (i / xs) % ys, z = i / (xs * ys);
     if (!t.in_data(x, y, z)) continue;
-    uint64_t gid = (t.bi[0] * 16ull + x) + (t.bi[1] * 16ull + y) * sy + (t.bi[2] * 16ull + z) * sz;
+    uint64_t gid = ((uint64_t)t.gs[0] + x) + ((uint64_t)t.gs[1] + y) * sy + ((uint64_t)t.gs[2] + z) * sz;
     T v = t.at(x, y, z);
     out[gid] = PROG ? Fp<T>::add(v, old[gid]) : v;
   }

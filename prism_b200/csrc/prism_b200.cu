@@ -1,0 +1,805 @@
+// prism_b200 C ABI: pipeline orchestration over the sm_100a kernels.
+//
+// One stream, no host round trip inside a pipeline: the REL range, the
+// auto-tune decisions, the per-level bounds, the chunk offsets and the output
+// size all stay in device memory and the host reads back one small status
+// block at the end of a call.  Device workspace is cached in the handle and
+// only grows.
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <string.h>
+#include <algorithm>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/prism_b200.h"
+#include "autotune.cuh"
+#include "bitplane.cuh"
+#include "geometry.h"
+#include "predict.cuh"
+#include "strategy.cuh"
+#include "zbpc.cuh"
+
+using namespace prism_b200;
+
+namespace {
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  cudaError_t ensure(size_t bytes) {
+    if (bytes <= cap) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    size_t want = bytes + bytes / 8 + 256;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e == cudaSuccess) cap = want;
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+  template <class U> U* as() const { return reinterpret_cast<U*>(p); }
+};
+
+// small device scratch block
+struct Small {
+  double range;
+  double eb;
+  uint64_t lossless_size;
+  uint64_t padded_size;
+  unsigned long long ticket;
+  int error_flag;
+  int pad;
+  uint64_t csbp[128];
+  unsigned char params[256];
+  StrategyState sstate;
+  StrategyBlock sblk[33];
+  double errors[16];
+};
+
+struct HostResult {
+  uint64_t padded_size;
+  int error_flag;
+  int pad;
+  unsigned char params[256];
+  double errors[16];
+};
+
+}  // namespace
+
+struct prism_handle {
+  DevBuf qc, planes, status, offs, bsum, part, wins, ranges, anchors, small, dev_in, dev_out, zero_anchors;
+  HostResult* host = nullptr;  // pinned
+  std::string err;
+  int sm_count = 148;
+};
+
+struct prism_prog {
+  prism_handle* h;
+  const uint8_t* cont;
+  uint64_t size;
+  int tsize;
+  Geometry g;
+  int mode;
+  double bound;
+  int steps;
+  StrategyState state;
+};
+
+static int fail(prism_handle* h, int code, const char* what, cudaError_t e = cudaSuccess) {
+  if (h) {
+    h->err = what;
+    if (e != cudaSuccess) {
+      h->err += ": ";
+      h->err += cudaGetErrorString(e);
+    }
+  }
+  return code;
+}
+
+#define CK(call)                                                   \
+  do {                                                             \
+    cudaError_t e_ = (call);                                       \
+    if (e_ != cudaSuccess) return fail(h, PRISM_ERR_CUDA, #call, e_); \
+  } while (0)
+
+#define CKA(call)                                                    \
+  do {                                                               \
+    cudaError_t e_ = (call);                                         \
+    if (e_ != cudaSuccess) return fail(h, PRISM_ERR_NOMEM, #call, e_); \
+  } while (0)
+
+static bool dims_ok(uint32_t nx, uint32_t ny, uint32_t nz) {
+  return nx >= 1 && ny >= 1 && nz >= 1 && (uint64_t)nx * ny * nz >= 2;
+}
+
+// code buffer: level-major codes plus the slack the reference's shuffle reads
+static uint64_t qc_len(const Geometry& g) {
+  int64_t end0 = (int64_t)g.n + g.align_dev;
+  int64_t last = g.sh_grid * (int64_t)kChunk + 64;
+  return g.anchors + (uint64_t)std::max(end0, last) + 64;
+}
+
+static Small* small(prism_handle* h) { return h->small.as<Small>(); }
+
+static int ensure_common(prism_handle* h, const Geometry& g) {
+  CKA(h->qc.ensure(qc_len(g) * sizeof(int32_t)));
+  CKA(h->planes.ensure(g.aligned_size + 64));
+  CKA(h->status.ensure((size_t)g.chunks * sizeof(unsigned long long)));
+  CKA(h->offs.ensure((size_t)g.chunks * sizeof(int64_t) + 64));
+  CKA(h->bsum.ensure(((size_t)g.chunks / kScanItems + 2) * sizeof(int64_t)));
+  CKA(h->anchors.ensure(g.anchors * 8 + 64));
+  CKA(h->small.ensure(sizeof(Small)));
+  return PRISM_OK;
+}
+
+template <class T>
+static const PredParams<T>* params_ptr(prism_handle* h) {
+  return reinterpret_cast<const PredParams<T>*>(small(h)->params);
+}
+
+// ---- stage launchers ----
+
+template <class T>
+static int launch_extrema(prism_handle* h, const T* in, uint64_t n, cudaStream_t st) {
+  int blocks = (int)std::min<uint64_t>((n + kExtThreads - 1) / kExtThreads, (uint64_t)h->sm_count * 4);
+  CKA(h->part.ensure(sizeof(T) * 2 * blocks));
+  extrema_kernel<T><<<blocks, kExtThreads, 0, st>>>(in, n, h->part.as<T>());
+  extrema_final_kernel<T><<<1, 32, 0, st>>>(h->part.as<T>(), blocks, &small(h)->range);
+  CK(cudaGetLastError());
+  return PRISM_OK;
+}
+
+__global__ void set_double_kernel(double* p, double v) { *p = v; }
+
+template <class T>
+static int launch_autotune_params(prism_handle* h, const T* in, const Geometry& g, int mode, double bound,
+                                  double rel_for_alpha, const uint8_t* force_flags_dev, cudaStream_t st) {
+  std::vector<SampleWindow> wins = sample_grid(g.nx, g.ny, g.nz);
+  int nwin = (int)wins.size();
+  double alpha = 1.0;
+  {
+    const double a1 = 2.0, a2 = 1.75, a3 = 1.5, a4 = 1.25, a5 = 1;
+    const double e1 = 1e-1, e2 = 1e-2, e3 = 1e-3, e4 = 1e-4, e5 = 1e-5;
+    double r = rel_for_alpha;  // InterpolationPredictor.cu:2248-2271
+    if (r >= e1) alpha = a1;
+    else if (r >= e2) alpha = a2 + (a1 - a2) * (r - e2) / (e1 - e2);
+    else if (r >= e3) alpha = a3 + (a2 - a3) * (r - e3) / (e2 - e3);
+    else if (r >= e4) alpha = a4 + (a3 - a4) * (r - e4) / (e3 - e4);
+    else if (r >= e5) alpha = a5 + (a4 - a5) * (r - e5) / (e4 - e5);
+    else alpha = a5;
+  }
+  Small* s = small(h);
+  if (!force_flags_dev) {
+    CKA(h->part.ensure(sizeof(T) * 15 * std::max(nwin, 1) + 64));
+    if (nwin > 0) {
+      CKA(h->wins.ensure(sizeof(SampleWindow) * nwin));
+      CK(cudaMemcpyAsync(h->wins.p, wins.data(), sizeof(SampleWindow) * nwin, cudaMemcpyHostToDevice, st));
+      autotune_kernel<T><<<dim3(nwin, 6), kAttThreads, 0, st>>>(in, g, h->wins.as<SampleWindow>(), h->part.as<T>());
+    }
+    params_kernel<T><<<1, 32, 0, st>>>(mode, bound, &s->range, alpha, h->part.as<T>(), nwin, nullptr, 4,
+                                       reinterpret_cast<PredParams<T>*>(s->params),
+                                       reinterpret_cast<T*>(s->errors), &s->eb);
+  } else {
+    params_kernel<T><<<1, 32, 0, st>>>(mode, bound, &s->range, alpha, nullptr, 0, force_flags_dev, 4,
+                                       reinterpret_cast<PredParams<T>*>(s->params), nullptr, &s->eb);
+  }
+  CK(cudaGetLastError());
+  return PRISM_OK;
+}
+
+static double alpha_of(double r) {
+  const double a1 = 2.0, a2 = 1.75, a3 = 1.5, a4 = 1.25, a5 = 1;
+  const double e1 = 1e-1, e2 = 1e-2, e3 = 1e-3, e4 = 1e-4, e5 = 1e-5;
+  if (r >= e1) return a1;
+  if (r >= e2) return a2 + (a1 - a2) * (r - e2) / (e1 - e2);
+  if (r >= e3) return a3 + (a2 - a3) * (r - e3) / (e2 - e3);
+  if (r >= e4) return a4 + (a3 - a4) * (r - e4) / (e3 - e4);
+  if (r >= e5) return a5 + (a4 - a5) * (r - e5) / (e4 - e5);
+  return a5;
+}
+
+// zero the code slots the predictor never writes but the shuffle reads
+static int zero_code_padding(prism_handle* h, const Geometry& g, cudaStream_t st) {
+  int32_t* qc = h->qc.as<int32_t>();
+  uint64_t c3 = g.grid[2] - g.grid[3], c2 = g.grid[1] - g.grid[2], c1 = g.grid[0] - g.grid[1];
+  uint64_t c0 = g.n - g.grid[0];
+  uint64_t segs[4][2] = {{g.anchors + c3, g.lm_prefix[2]},
+                         {g.lm_prefix[2] + c2, g.lm_prefix[1]},
+                         {g.lm_prefix[1] + c1, g.lm_prefix[0]},
+                         {g.lm_prefix[0] + c0, qc_len(g)}};
+  for (auto& s : segs)
+    if (s[1] > s[0]) CK(cudaMemsetAsync(qc + s[0], 0, (s[1] - s[0]) * sizeof(int32_t), st));
+  return PRISM_OK;
+}
+
+static int launch_bitshuffle(prism_handle* h, const int32_t* qc, const Geometry& g, int nb, uint8_t* planes,
+                             cudaStream_t st) {
+  int64_t start_last = (g.sh_grid - 1) * (int64_t)kChunk;
+  ShufPlan plan = make_shuf_plan(g, start_last);
+  ByteRange rng[160];
+  int nr = fill_ranges(g, plan, rng, 160);
+  if (nr > 0) {
+    CKA(h->ranges.ensure(sizeof(rng)));
+    CK(cudaMemcpyAsync(h->ranges.p, rng, sizeof(ByteRange) * nr, cudaMemcpyHostToDevice, st));
+    leftover_fill_kernel<<<nr, 256, 0, st>>>(planes, qc, g, h->ranges.as<ByteRange>(), nr);
+  }
+  const int32_t* codes = qc + g.anchors;
+  bool last_last = last_block_lands_last(g);
+  if (!last_last) shuffle_last_block_kernel<<<1, 512, 0, st>>>(codes, planes, g, nb, g.aligned_size);
+  if (plan.items > 0) {
+    int64_t blocks = (plan.items + kShufWarps - 1) / kShufWarps;
+    bitshuffle_kernel<<<(unsigned)blocks, kShufWarps * 32, 0, st>>>(codes, planes, g, plan, nb);
+  }
+  if (last_last) shuffle_last_block_kernel<<<1, 512, 0, st>>>(codes, planes, g, nb, g.aligned_size);
+  CK(cudaGetLastError());
+  return PRISM_OK;
+}
+
+static int launch_inverse(prism_handle* h, const uint8_t* planes, const Geometry& g, int nb, const int* dbegin,
+                          const int* dend, int32_t* qc, cudaStream_t st) {
+  int64_t start_last = (g.sh_grid - 1) * (int64_t)kChunk;
+  // positions from the last block on are only partly written: start from 0
+  uint64_t from = g.anchors + (uint64_t)start_last;
+  uint64_t to = qc_len(g);
+  if (to > from) CK(cudaMemsetAsync(qc + from, 0, (to - from) * sizeof(int32_t), st));
+  ShufPlan plan = make_shuf_plan(g, start_last);
+  int32_t* codes = qc + g.anchors;
+  if (plan.items > 0) {
+    int64_t blocks = (plan.items + kShufWarps - 1) / kShufWarps;
+    inverse_bitshuffle_kernel<<<(unsigned)blocks, kShufWarps * 32, 0, st>>>(planes, codes, g, plan, nb, dbegin, dend);
+  }
+  inverse_last_block_kernel<<<1, 512, 0, st>>>(planes, codes, g, nb, dbegin, dend, g.aligned_size);
+  CK(cudaGetLastError());
+  return PRISM_OK;
+}
+
+static int launch_encode(prism_handle* h, const uint8_t* planes, const Geometry& g, uint8_t* stream,
+                         cudaStream_t st) {
+  Small* s = small(h);
+  CK(cudaMemsetAsync(h->status.p, 0, (size_t)g.chunks * sizeof(unsigned long long), st));
+  CK(cudaMemsetAsync(&s->ticket, 0, sizeof(unsigned long long), st));
+  CK(cudaMemsetAsync(&s->error_flag, 0, sizeof(int), st));
+  size_t smem = sizeof(EncodeShared);
+  static bool attr_set = false;
+  if (!attr_set) {
+    CK(cudaFuncSetAttribute(zbpc_encode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr_set = true;
+  }
+  int blocks = (int)std::min<int64_t>(g.chunks, (int64_t)h->sm_count * 4);
+  zbpc_encode_kernel<<<blocks, kZThreads, smem, st>>>(planes, g, stream, h->status.as<unsigned long long>(),
+                                                      &s->ticket, s->csbp, &s->lossless_size, &s->error_flag,
+                                                      (long long)1 << 22);
+  zbpc_finish_kernel<<<1, 32, 0, st>>>(stream, g, &s->lossless_size, &s->padded_size);
+  CK(cudaGetLastError());
+  return PRISM_OK;
+}
+
+static int launch_decode(prism_handle* h, const uint8_t* stream, uint64_t stream_bytes, const Geometry& g,
+                         const int* dbegin, const int* dend, uint8_t* planes, cudaStream_t st) {
+  Small* s = small(h);
+  const uint16_t* sizes = reinterpret_cast<const uint16_t*>(stream + 8);
+  int64_t nblk = (g.chunks + kScanItems - 1) / kScanItems;
+  scan_sizes_block<<<(unsigned)nblk, 1024, 0, st>>>(sizes, g.chunks, h->offs.as<int64_t>(), h->bsum.as<int64_t>());
+  scan_block_sums<<<1, 32, 0, st>>>(h->bsum.as<int64_t>(), nblk);
+  scan_add<<<(unsigned)((g.chunks + 255) / 256), 256, 0, st>>>(h->offs.as<int64_t>(), g.chunks, h->bsum.as<int64_t>());
+  CK(cudaMemsetAsync(&s->error_flag, 0, sizeof(int), st));
+  size_t smem = sizeof(DecodeShared);
+  static bool attr_set = false;
+  if (!attr_set) {
+    CK(cudaFuncSetAttribute(zbpc_decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr_set = true;
+  }
+  int blocks = (int)std::min<int64_t>(g.chunks, (int64_t)h->sm_count * 8);
+  zbpc_decode_kernel<<<blocks, kZThreads, smem, st>>>(stream, stream_bytes, h->offs.as<int64_t>(), g, planes,
+                                                      dbegin, dend, &s->error_flag);
+  CK(cudaGetLastError());
+  return PRISM_OK;
+}
+
+// trailer (compress_merge, compressor.cu:139-151): use_md[4], reverse[4],
+// double range, size_t comp_size_bp[4][32], anchors
+template <class T>
+__global__ void trailer_kernel(uint8_t* stream, const uint64_t* padded, const PredParams<T>* p, const double* range,
+                               const uint64_t* csbp, const T* anchors, uint64_t nanchors) {
+  uint8_t* tr = stream + *padded;
+  uint64_t total = 1040 + nanchors * sizeof(T);
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
+    uint8_t v;
+    if (i < 4) v = p->use_md[i];
+    else if (i < 8) v = p->reverse[i - 4];
+    else if (i < 16) v = reinterpret_cast<const uint8_t*>(range)[i - 8];
+    else if (i < 1040) v = reinterpret_cast<const uint8_t*>(csbp)[i - 16];
+    else v = reinterpret_cast<const uint8_t*>(anchors)[i - 1040];
+    tr[i] = v;
+  }
+}
+
+static int finish(prism_handle* h, cudaStream_t st) {
+  Small* s = small(h);
+  CK(cudaMemcpyAsync(&h->host->padded_size, &s->padded_size, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(&h->host->error_flag, &s->error_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(h->host->params, s->params, sizeof(s->params), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(h->host->errors, s->errors, sizeof(s->errors), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (h->host->error_flag == 1) return fail(h, PRISM_ERR_TIMEOUT, "look-back wait exceeded its limit");
+  if (h->host->error_flag == 2) return fail(h, PRISM_ERR_CORRUPT, "corrupt lossless chunk");
+  return PRISM_OK;
+}
+
+template <class T>
+static int compress_t(prism_handle* h, const T* in, const Geometry& g, int mode, double bound, int nb,
+                      uint8_t* out, uint64_t cap, uint64_t* out_size, uint8_t* flags_out, cudaStream_t st) {
+  int rc = ensure_common(h, g);
+  if (rc) return rc;
+  uint64_t need = 8 + 2 * (uint64_t)g.chunks + g.aligned_size + 8 + g.header_size;
+  if (cap < need) return fail(h, PRISM_ERR_ARG, "output capacity below prism_max_container_size");
+  Small* s = small(h);
+  if (mode == 1) {
+    rc = launch_extrema<T>(h, in, g.n, st);
+    if (rc) return rc;
+  } else {
+    set_double_kernel<<<1, 1, 0, st>>>(&s->range, 1.0);
+  }
+  rc = launch_autotune_params<T>(h, in, g, mode, bound, mode == 1 ? bound : 0.0, nullptr, st);
+  if (rc) return rc;
+  rc = zero_code_padding(h, g, st);
+  if (rc) return rc;
+  predict_compress_kernel<T><<<(unsigned)g.anchors, kPredThreads, 0, st>>>(in, g, params_ptr<T>(h), h->anchors.as<T>(),
+                                                                            h->qc.as<int32_t>());
+  CK(cudaGetLastError());
+  rc = launch_bitshuffle(h, h->qc.as<int32_t>(), g, nb, h->planes.as<uint8_t>(), st);
+  if (rc) return rc;
+  rc = launch_encode(h, h->planes.as<uint8_t>(), g, out, st);
+  if (rc) return rc;
+  trailer_kernel<T><<<64, 256, 0, st>>>(out, &s->padded_size, params_ptr<T>(h), &s->range, s->csbp,
+                                        h->anchors.as<T>(), g.anchors);
+  CK(cudaGetLastError());
+  rc = finish(h, st);
+  if (rc) return rc;
+  *out_size = h->host->padded_size + g.header_size;
+  if (flags_out) {
+    const PredParams<T>* p = reinterpret_cast<const PredParams<T>*>(h->host->params);
+    for (int l = 0; l < 4; ++l) { flags_out[l] = p->use_md[l]; flags_out[4 + l] = p->reverse[l]; }
+  }
+  return PRISM_OK;
+}
+
+template <class T>
+static int decompress_t(prism_handle* h, const uint8_t* cont, uint64_t size, const Geometry& g, int mode,
+                        double bound, T* out, cudaStream_t st) {
+  int rc = ensure_common(h, g);
+  if (rc) return rc;
+  if (size < g.header_size + 8 + 2 * (uint64_t)g.chunks) return fail(h, PRISM_ERR_CORRUPT, "container too small");
+  const uint8_t* tr = cont + (size - g.header_size);
+  Small* s = small(h);
+  CK(cudaMemcpyAsync(&s->range, tr + 8, sizeof(double), cudaMemcpyDeviceToDevice, st));
+  params_kernel<T><<<1, 32, 0, st>>>(mode, bound, &s->range, alpha_of(mode == 1 ? bound : 0.0), nullptr, 0, tr, 4,
+                                     reinterpret_cast<PredParams<T>*>(s->params), nullptr, &s->eb);
+  rc = launch_decode(h, cont, size - g.header_size, g, nullptr, nullptr, h->planes.as<uint8_t>(), st);
+  if (rc) return rc;
+  rc = launch_inverse(h, h->planes.as<uint8_t>(), g, 0 /*SM*/, nullptr, nullptr, h->qc.as<int32_t>(), st);
+  if (rc) return rc;
+  reconstruct_kernel<T, false><<<(unsigned)g.anchors, kPredThreads, 0, st>>>(
+      h->qc.as<int32_t>(), reinterpret_cast<const T*>(tr + 1040), g, params_ptr<T>(h), nullptr, out);
+  CK(cudaGetLastError());
+  return finish(h, st);
+}
+
+// ---- exported API (C linkage comes from the declarations in prism_b200.h) ----
+
+int prism_create(prism_handle** out) {
+  if (!out) return PRISM_ERR_ARG;
+  prism_handle* h = new (std::nothrow) prism_handle();
+  if (!h) return PRISM_ERR_NOMEM;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess) e = cudaMallocHost((void**)&h->host, sizeof(HostResult));
+  if (e != cudaSuccess) {
+    delete h;
+    return PRISM_ERR_CUDA;
+  }
+  *out = h;
+  return PRISM_OK;
+}
+
+void prism_destroy(prism_handle* h) {
+  if (!h) return;
+  DevBuf* bufs[] = {&h->qc, &h->planes, &h->status, &h->offs, &h->bsum, &h->part, &h->wins, &h->ranges,
+                    &h->anchors, &h->small, &h->dev_in, &h->dev_out, &h->zero_anchors};
+  for (DevBuf* b : bufs) b->release();
+  if (h->host) cudaFreeHost(h->host);
+  delete h;
+}
+
+const char* prism_last_error(const prism_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+uint64_t prism_max_container_size(uint32_t nx, uint32_t ny, uint32_t nz, int dtype_size) {
+  Geometry g;
+  make_geometry(nx, ny, nz, dtype_size, &g);
+  return 8 + 2 * (uint64_t)g.chunks + g.aligned_size + 8 + g.header_size;
+}
+
+uint64_t prism_plane_buffer_size(uint32_t nx, uint32_t ny, uint32_t nz) {
+  Geometry g;
+  make_geometry(nx, ny, nz, 4, &g);
+  return g.aligned_size;
+}
+
+uint64_t prism_trailer_size(uint32_t nx, uint32_t ny, uint32_t nz, int dtype_size) {
+  Geometry g;
+  make_geometry(nx, ny, nz, dtype_size, &g);
+  return g.header_size;
+}
+
+uint64_t prism_code_buffer_len(uint32_t nx, uint32_t ny, uint32_t nz) {
+  Geometry g;
+  make_geometry(nx, ny, nz, 4, &g);
+  return qc_len(g);
+}
+
+int prism_compress(prism_handle* h, const void* d_in, int dtype_size, uint32_t nx, uint32_t ny, uint32_t nz,
+                   int mode, double bound, int progressive, void* d_out, uint64_t out_capacity,
+                   uint64_t* out_size, uint8_t flags_out[8], void* stream) {
+  if (!h || !d_in || !d_out || !out_size) return PRISM_ERR_ARG;
+  if ((dtype_size != 4 && dtype_size != 8) || !dims_ok(nx, ny, nz) || !(bound > 0) || (mode != 0 && mode != 1))
+    return fail(h, PRISM_ERR_ARG, "bad dtype, dimensions, mode or bound");
+  Geometry g;
+  make_geometry(nx, ny, nz, dtype_size, &g);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (dtype_size == 4)
+    return compress_t<float>(h, (const float*)d_in, g, mode, bound, progressive ? 1 : 0, (uint8_t*)d_out,
+                             out_capacity, out_size, flags_out, st);
+  return compress_t<double>(h, (const double*)d_in, g, mode, bound, progressive ? 1 : 0, (uint8_t*)d_out,
+                            out_capacity, out_size, flags_out, st);
+}
+
+int prism_compress_host(prism_handle* h, const void* h_in, int dtype_size, uint32_t nx, uint32_t ny, uint32_t nz,
+                        int mode, double bound, int progressive, void* h_out, uint64_t out_capacity,
+                        uint64_t* out_size, void* stream) {
+  if (!h || !h_in || !h_out || !out_size) return PRISM_ERR_ARG;
+  if ((dtype_size != 4 && dtype_size != 8) || !dims_ok(nx, ny, nz)) return fail(h, PRISM_ERR_ARG, "bad dims");
+  uint64_t n = (uint64_t)nx * ny * nz;
+  uint64_t cap = prism_max_container_size(nx, ny, nz, dtype_size);
+  cudaStream_t st = (cudaStream_t)stream;
+  CKA(h->dev_in.ensure(n * dtype_size));
+  CKA(h->dev_out.ensure(cap));
+  CK(cudaMemcpyAsync(h->dev_in.p, h_in, n * dtype_size, cudaMemcpyHostToDevice, st));
+  uint64_t size = 0;
+  int rc = prism_compress(h, h->dev_in.p, dtype_size, nx, ny, nz, mode, bound, progressive, h->dev_out.p, cap,
+                          &size, nullptr, stream);
+  if (rc) return rc;
+  if (size > out_capacity) return fail(h, PRISM_ERR_ARG, "host output buffer too small");
+  CK(cudaMemcpyAsync(h_out, h->dev_out.p, size, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  *out_size = size;
+  return PRISM_OK;
+}
+
+int prism_decompress(prism_handle* h, const void* d_container, uint64_t size, int dtype_size, uint32_t nx,
+                     uint32_t ny, uint32_t nz, int mode, double bound, void* d_out, void* stream) {
+  if (!h || !d_container || !d_out) return PRISM_ERR_ARG;
+  if ((dtype_size != 4 && dtype_size != 8) || !dims_ok(nx, ny, nz) || !(bound > 0) || (mode != 0 && mode != 1))
+    return fail(h, PRISM_ERR_ARG, "bad dtype, dimensions, mode or bound");
+  Geometry g;
+  make_geometry(nx, ny, nz, dtype_size, &g);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (dtype_size == 4)
+    return decompress_t<float>(h, (const uint8_t*)d_container, size, g, mode, bound, (float*)d_out, st);
+  return decompress_t<double>(h, (const uint8_t*)d_container, size, g, mode, bound, (double*)d_out, st);
+}
+
+int prism_decompress_host(prism_handle* h, const void* h_container, uint64_t size, int dtype_size, uint32_t nx,
+                          uint32_t ny, uint32_t nz, int mode, double bound, void* h_out, void* stream) {
+  if (!h || !h_container || !h_out) return PRISM_ERR_ARG;
+  if ((dtype_size != 4 && dtype_size != 8) || !dims_ok(nx, ny, nz)) return fail(h, PRISM_ERR_ARG, "bad dims");
+  uint64_t n = (uint64_t)nx * ny * nz;
+  cudaStream_t st = (cudaStream_t)stream;
+  CKA(h->dev_in.ensure(size));
+  CKA(h->dev_out.ensure(n * dtype_size));
+  CK(cudaMemcpyAsync(h->dev_in.p, h_container, size, cudaMemcpyHostToDevice, st));
+  int rc = prism_decompress(h, h->dev_in.p, size, dtype_size, nx, ny, nz, mode, bound, h->dev_out.p, stream);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(h_out, h->dev_out.p, n * dtype_size, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return PRISM_OK;
+}
+
+int prism_progressive_open(prism_handle* h, const void* d_container, uint64_t size, int dtype_size, uint32_t nx,
+                           uint32_t ny, uint32_t nz, int mode, double bound, prism_prog** out) {
+  if (!h || !d_container || !out) return PRISM_ERR_ARG;
+  if ((dtype_size != 4 && dtype_size != 8) || !dims_ok(nx, ny, nz) || !(bound > 0) || (mode != 0 && mode != 1))
+    return fail(h, PRISM_ERR_ARG, "bad dtype, dimensions, mode or bound");
+  prism_prog* p = new (std::nothrow) prism_prog();
+  if (!p) return PRISM_ERR_NOMEM;
+  p->h = h;
+  p->cont = (const uint8_t*)d_container;
+  p->size = size;
+  p->tsize = dtype_size;
+  make_geometry(nx, ny, nz, dtype_size, &p->g);
+  if (size < p->g.header_size + 8 + 2 * (uint64_t)p->g.chunks) {
+    delete p;
+    return fail(h, PRISM_ERR_CORRUPT, "container too small");
+  }
+  p->mode = mode;
+  p->bound = bound;
+  p->steps = 0;
+  memset(&p->state, 0, sizeof(p->state));
+  p->state.maxlevel = 4;
+  *out = p;
+  return PRISM_OK;
+}
+
+template <class T>
+static int progressive_step_t(prism_prog* p, double target, T* values, cudaStream_t st) {
+  prism_handle* h = p->h;
+  const Geometry& g = p->g;
+  int rc = ensure_common(h, g);
+  if (rc) return rc;
+  CKA(h->zero_anchors.ensure(g.anchors * sizeof(T) + 64));
+  Small* s = small(h);
+  const uint8_t* tr = p->cont + (p->size - g.header_size);
+  bool first = p->steps == 0;
+  CK(cudaMemcpyAsync(&s->range, tr + 8, sizeof(double), cudaMemcpyDeviceToDevice, st));
+  CK(cudaMemcpyAsync(&s->sstate, &p->state, sizeof(StrategyState), cudaMemcpyHostToDevice, st));
+  // strategy (findStrategy_h) from the container's cumulative plane sizes
+  const uint64_t* csbp = reinterpret_cast<const uint64_t*>(tr + 16);
+  strategy_search_kernel<<<33, 1024, 0, st>>>(csbp, p->mode, p->bound, target, &s->range, s->sblk);
+  strategy_finish_kernel<<<1, 32, 0, st>>>(s->sblk, p->mode, p->bound, target, &s->range, &s->sstate);
+  // parameters with maxlevel from the strategy
+  params_kernel<T><<<1, 32, 0, st>>>(p->mode, p->bound, &s->range, alpha_of(p->mode == 1 ? p->bound : 0.0), nullptr,
+                                     0, tr, 4, reinterpret_cast<PredParams<T>*>(s->params), nullptr, &s->eb);
+  CK(cudaMemcpyAsync(&reinterpret_cast<PredParams<T>*>(s->params)->maxlevel, &s->sstate.maxlevel, sizeof(int),
+                     cudaMemcpyDeviceToDevice, st));
+  CK(cudaMemsetAsync(h->planes.p, 0, g.aligned_size, st));
+  rc = launch_decode(h, p->cont, p->size - g.header_size, g, s->sstate.begin, s->sstate.end,
+                     h->planes.as<uint8_t>(), st);
+  if (rc) return rc;
+  rc = launch_inverse(h, h->planes.as<uint8_t>(), g, 1 /*NB*/, s->sstate.begin, s->sstate.end, h->qc.as<int32_t>(), st);
+  if (rc) return rc;
+  if (first) {
+    reconstruct_kernel<T, false><<<(unsigned)g.anchors, kPredThreads, 0, st>>>(
+        h->qc.as<int32_t>(), reinterpret_cast<const T*>(tr + 1040), g, params_ptr<T>(h), nullptr, values);
+  } else {
+    CK(cudaMemsetAsync(h->zero_anchors.p, 0, g.anchors * sizeof(T), st));
+    reconstruct_kernel<T, true><<<(unsigned)g.anchors, kPredThreads, 0, st>>>(
+        h->qc.as<int32_t>(), h->zero_anchors.as<T>(), g, params_ptr<T>(h), values, values);
+  }
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(&p->state, &s->sstate, sizeof(StrategyState), cudaMemcpyDeviceToHost, st));
+  rc = finish(h, st);
+  if (rc) return rc;
+  p->steps++;
+  return PRISM_OK;
+}
+
+int prism_progressive_step(prism_prog* p, double target_error, void* d_values, void* stream) {
+  if (!p || !d_values || !(target_error > 0)) return PRISM_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (p->tsize == 4) return progressive_step_t<float>(p, target_error, (float*)d_values, st);
+  return progressive_step_t<double>(p, target_error, (double*)d_values, st);
+}
+
+int prism_progressive_state(const prism_prog* p, int begin[4], int end[4], int* maxlevel, uint64_t* loaded) {
+  if (!p) return PRISM_ERR_ARG;
+  for (int i = 0; i < 4; ++i) {
+    if (begin) begin[i] = p->state.begin[i];
+    if (end) end[i] = p->state.end[i];
+  }
+  if (maxlevel) *maxlevel = p->state.maxlevel;
+  if (loaded) *loaded = 0;
+  return PRISM_OK;
+}
+
+void prism_progressive_close(prism_prog* p) { delete p; }
+
+// ---- stage entry points ----
+
+int prism_extrema(prism_handle* h, const void* d_in, int dtype_size, uint64_t n, double* range_out, void* stream) {
+  if (!h || !d_in || !range_out || n == 0) return PRISM_ERR_ARG;
+  CKA(h->small.ensure(sizeof(Small)));
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc = dtype_size == 4 ? launch_extrema<float>(h, (const float*)d_in, n, st)
+                           : launch_extrema<double>(h, (const double*)d_in, n, st);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(range_out, &small(h)->range, sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return PRISM_OK;
+}
+
+int prism_autotune(prism_handle* h, const void* d_in, int dtype_size, uint32_t nx, uint32_t ny, uint32_t nz,
+                   double* errors_out, uint8_t flags_out[8], void* stream) {
+  if (!h || !d_in || !dims_ok(nx, ny, nz)) return PRISM_ERR_ARG;
+  Geometry g;
+  make_geometry(nx, ny, nz, dtype_size, &g);
+  int rc = ensure_common(h, g);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  set_double_kernel<<<1, 1, 0, st>>>(&small(h)->range, 1.0);
+  rc = dtype_size == 4 ? launch_autotune_params<float>(h, (const float*)d_in, g, 0, 1.0, 0.0, nullptr, st)
+                       : launch_autotune_params<double>(h, (const double*)d_in, g, 0, 1.0, 0.0, nullptr, st);
+  if (rc) return rc;
+  rc = finish(h, st);
+  if (rc) return rc;
+  for (int k = 0; k < 15; ++k) {
+    if (!errors_out) break;
+    errors_out[k] = dtype_size == 4 ? (double)reinterpret_cast<const float*>(h->host->errors)[k]
+                                    : h->host->errors[k];
+  }
+  if (flags_out) {
+    const uint8_t* md = dtype_size == 4 ? reinterpret_cast<const PredParams<float>*>(h->host->params)->use_md
+                                        : reinterpret_cast<const PredParams<double>*>(h->host->params)->use_md;
+    const uint8_t* rv = dtype_size == 4 ? reinterpret_cast<const PredParams<float>*>(h->host->params)->reverse
+                                        : reinterpret_cast<const PredParams<double>*>(h->host->params)->reverse;
+    for (int l = 0; l < 4; ++l) { flags_out[l] = md[l]; flags_out[4 + l] = rv[l]; }
+  }
+  return PRISM_OK;
+}
+
+template <class T>
+static int predict_stage_t(prism_handle* h, const T* in, const Geometry& g, double eb, double rel_eb,
+                           const uint8_t* flags, int32_t* codes, T* anchors, cudaStream_t st) {
+  int rc = ensure_common(h, g);
+  if (rc) return rc;
+  Small* s = small(h);
+  CK(cudaMemcpyAsync(s->params + 200, flags, 8, cudaMemcpyHostToDevice, st));
+  set_double_kernel<<<1, 1, 0, st>>>(&s->range, 1.0);
+  params_kernel<T><<<1, 32, 0, st>>>(0, eb, &s->range, alpha_of(rel_eb), nullptr, 0, s->params + 200, 4,
+                                     reinterpret_cast<PredParams<T>*>(s->params), nullptr, &s->eb);
+  predict_compress_kernel<T><<<(unsigned)g.anchors, kPredThreads, 0, st>>>(in, g, params_ptr<T>(h), anchors, codes);
+  CK(cudaGetLastError());
+  return finish(h, st);
+}
+
+int prism_predict(prism_handle* h, const void* d_in, int dtype_size, uint32_t nx, uint32_t ny, uint32_t nz,
+                  double eb, double rel_eb, const uint8_t flags[8], int32_t* d_codes, void* d_anchors, void* stream) {
+  if (!h || !d_in || !d_codes || !d_anchors || !flags || !dims_ok(nx, ny, nz) || !(eb > 0)) return PRISM_ERR_ARG;
+  Geometry g;
+  make_geometry(nx, ny, nz, dtype_size, &g);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (dtype_size == 4)
+    return predict_stage_t<float>(h, (const float*)d_in, g, eb, rel_eb, flags, d_codes, (float*)d_anchors, st);
+  return predict_stage_t<double>(h, (const double*)d_in, g, eb, rel_eb, flags, d_codes, (double*)d_anchors, st);
+}
+
+template <class T>
+static int reconstruct_stage_t(prism_handle* h, const int32_t* codes, const T* anchors, const Geometry& g, double eb,
+                               double rel_eb, const uint8_t* flags, int maxlevel, const T* old, T* out,
+                               cudaStream_t st) {
+  int rc = ensure_common(h, g);
+  if (rc) return rc;
+  Small* s = small(h);
+  CK(cudaMemcpyAsync(s->params + 200, flags, 8, cudaMemcpyHostToDevice, st));
+  set_double_kernel<<<1, 1, 0, st>>>(&s->range, 1.0);
+  params_kernel<T><<<1, 32, 0, st>>>(0, eb, &s->range, alpha_of(rel_eb), nullptr, 0, s->params + 200, maxlevel,
+                                     reinterpret_cast<PredParams<T>*>(s->params), nullptr, &s->eb);
+  if (old)
+    reconstruct_kernel<T, true><<<(unsigned)g.anchors, kPredThreads, 0, st>>>(codes, anchors, g, params_ptr<T>(h), old, out);
+  else
+    reconstruct_kernel<T, false><<<(unsigned)g.anchors, kPredThreads, 0, st>>>(codes, anchors, g, params_ptr<T>(h), nullptr, out);
+  CK(cudaGetLastError());
+  return finish(h, st);
+}
+
+int prism_reconstruct(prism_handle* h, const int32_t* d_codes, const void* d_anchors, int dtype_size, uint32_t nx,
+                      uint32_t ny, uint32_t nz, double eb, double rel_eb, const uint8_t flags[8], int maxlevel,
+                      const void* d_old, void* d_out, void* stream) {
+  if (!h || !d_codes || !d_anchors || !d_out || !flags || !dims_ok(nx, ny, nz) || !(eb > 0)) return PRISM_ERR_ARG;
+  Geometry g;
+  make_geometry(nx, ny, nz, dtype_size, &g);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (dtype_size == 4)
+    return reconstruct_stage_t<float>(h, d_codes, (const float*)d_anchors, g, eb, rel_eb, flags, maxlevel,
+                                      (const float*)d_old, (float*)d_out, st);
+  return reconstruct_stage_t<double>(h, d_codes, (const double*)d_anchors, g, eb, rel_eb, flags, maxlevel,
+                                     (const double*)d_old, (double*)d_out, st);
+}
+
+int prism_bitshuffle(prism_handle* h, const int32_t* d_codes, uint32_t nx, uint32_t ny, uint32_t nz, int progressive,
+                     uint8_t* d_planes, void* stream) {
+  if (!h || !d_codes || !d_planes || !dims_ok(nx, ny, nz)) return PRISM_ERR_ARG;
+  Geometry g;
+  make_geometry(nx, ny, nz, 4, &g);
+  int rc = ensure_common(h, g);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  rc = launch_bitshuffle(h, d_codes, g, progressive ? 1 : 0, d_planes, st);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(st));
+  return PRISM_OK;
+}
+
+static int host_range(prism_handle* h, const int* hb, const int* he, cudaStream_t st, int** db, int** de) {
+  *db = *de = nullptr;
+  if (!hb) return PRISM_OK;
+  Small* s = small(h);
+  StrategyState tmp;
+  memset(&tmp, 0, sizeof(tmp));
+  for (int i = 0; i < 4; ++i) { tmp.begin[i] = hb[i]; tmp.end[i] = he[i]; }
+  CK(cudaMemcpyAsync(&s->sstate, &tmp, sizeof(tmp), cudaMemcpyHostToDevice, st));
+  *db = s->sstate.begin;
+  *de = s->sstate.end;
+  return PRISM_OK;
+}
+
+int prism_inverse_bitshuffle(prism_handle* h, const uint8_t* d_planes, uint32_t nx, uint32_t ny, uint32_t nz,
+                             int progressive, const int begin[4], const int end[4], int32_t* d_codes, void* stream) {
+  if (!h || !d_codes || !d_planes || !dims_ok(nx, ny, nz) || (!begin) != (!end)) return PRISM_ERR_ARG;
+  Geometry g;
+  make_geometry(nx, ny, nz, 4, &g);
+  int rc = ensure_common(h, g);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  int *db, *de;
+  rc = host_range(h, begin, end, st, &db, &de);
+  if (rc) return rc;
+  rc = launch_inverse(h, d_planes, g, progressive ? 1 : 0, db, de, d_codes, st);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(st));
+  return PRISM_OK;
+}
+
+int prism_lossless_encode(prism_handle* h, const uint8_t* d_planes, uint32_t nx, uint32_t ny, uint32_t nz,
+                          uint8_t* d_stream, uint64_t capacity, uint64_t* size_out, uint64_t comp_size_bp[128],
+                          void* stream) {
+  if (!h || !d_planes || !d_stream || !size_out || !dims_ok(nx, ny, nz)) return PRISM_ERR_ARG;
+  Geometry g;
+  make_geometry(nx, ny, nz, 4, &g);
+  if (capacity < 8 + 2 * (uint64_t)g.chunks + g.aligned_size + 8) return fail(h, PRISM_ERR_ARG, "capacity");
+  int rc = ensure_common(h, g);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  rc = launch_encode(h, d_planes, g, d_stream, st);
+  if (rc) return rc;
+  if (comp_size_bp) CK(cudaMemcpyAsync(comp_size_bp, small(h)->csbp, 1024, cudaMemcpyDeviceToHost, st));
+  rc = finish(h, st);
+  if (rc) return rc;
+  *size_out = h->host->padded_size;
+  return PRISM_OK;
+}
+
+int prism_lossless_decode(prism_handle* h, const uint8_t* d_stream, uint32_t nx, uint32_t ny, uint32_t nz,
+                          const int begin[4], const int end[4], uint8_t* d_planes, void* stream) {
+  if (!h || !d_planes || !d_stream || !dims_ok(nx, ny, nz) || (!begin) != (!end)) return PRISM_ERR_ARG;
+  Geometry g;
+  make_geometry(nx, ny, nz, 4, &g);
+  int rc = ensure_common(h, g);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  int *db, *de;
+  rc = host_range(h, begin, end, st, &db, &de);
+  if (rc) return rc;
+  rc = launch_decode(h, d_stream, ~0ull, g, db, de, d_planes, st);
+  if (rc) return rc;
+  return finish(h, st);
+}
+
+int prism_find_strategy(prism_handle* h, const uint64_t comp_size_bp[128], double eb, double target_error,
+                        int begin[4], int end[4], int* maxlevel, void* stream) {
+  if (!h || !comp_size_bp || !begin || !end || !maxlevel || !(eb > 0)) return PRISM_ERR_ARG;
+  CKA(h->small.ensure(sizeof(Small)));
+  CKA(h->part.ensure(1024 + 64));
+  cudaStream_t st = (cudaStream_t)stream;
+  Small* s = small(h);
+  StrategyState tmp;
+  for (int i = 0; i < 4; ++i) { tmp.begin[i] = begin[i]; tmp.end[i] = end[i]; }
+  tmp.maxlevel = *maxlevel;
+  CK(cudaMemcpyAsync(&s->sstate, &tmp, sizeof(tmp), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(h->part.p, comp_size_bp, 1024, cudaMemcpyHostToDevice, st));
+  set_double_kernel<<<1, 1, 0, st>>>(&s->range, 1.0);
+  strategy_search_kernel<<<33, 1024, 0, st>>>(h->part.as<uint64_t>(), 0, eb, target_error, &s->range, s->sblk);
+  strategy_finish_kernel<<<1, 32, 0, st>>>(s->sblk, 0, eb, target_error, &s->range, &s->sstate);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(&tmp, &s->sstate, sizeof(tmp), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  for (int i = 0; i < 4; ++i) { begin[i] = tmp.begin[i]; end[i] = tmp.end[i]; }
+  *maxlevel = tmp.maxlevel;
+  return PRISM_OK;
+}
+

@@ -86,7 +86,9 @@ __device__ __forceinline__ int block_excl_scan(int v, int* scratch, int* total) 
 
 struct EncodeShared {
   uint8_t in[kChunk];
-  uint8_t out[kChunk + 64];
+  // payload staging: nonzero bytes (< osize) plus up to 2048 + 256 + 32 + 6
+  // bitmap bytes before the size check can reject the encoding
+  uint8_t out[kChunk + 2048 + 512];
   uint8_t bm0[2048];
   uint8_t bm1[256];
   uint8_t bm2[32];
@@ -224,7 +226,10 @@ zbpc_encode_kernel(const uint8_t* __restrict__ planes, Geometry g, uint8_t* __re
           if (k >= 0) {
             do {
               v = atomicAdd(&status[k], 0ull);
-              if (v == 0 && ++spins > spin_limit) { atomicExch(error_flag, 1); v = kInc; }
+              if (v == 0) {
+                if (++spins > spin_limit) { atomicExch(error_flag, 1); v = kInc; }
+                else __nanosleep(64);
+              }
             } while (v == 0);
           }
           unsigned inc_mask = __ballot_sync(0xffffffffu, (v >> 62) == 2);
@@ -363,9 +368,9 @@ __device__ __forceinline__ int popc_bytes_block(const uint8_t* b, int n, int* sc
 // host planes [begin[3-l], end[3-l]) like zbpc_decode_progressive
 // (zbpc.cu:420-423).  Returns per-chunk errors through error_flag.
 __global__ void __launch_bounds__(kZThreads)
-zbpc_decode_kernel(const uint8_t* __restrict__ stream, const int64_t* __restrict__ offs, Geometry g,
-                   uint8_t* __restrict__ planes, const int* __restrict__ begin, const int* __restrict__ end,
-                   int* __restrict__ error_flag) {
+zbpc_decode_kernel(const uint8_t* __restrict__ stream, uint64_t stream_bytes, const int64_t* __restrict__ offs,
+                   Geometry g, uint8_t* __restrict__ planes, const int* __restrict__ begin,
+                   const int* __restrict__ end, int* __restrict__ error_flag) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   DecodeShared& sh = *reinterpret_cast<DecodeShared*>(smem_raw);
   const int tid = threadIdx.x;
@@ -381,6 +386,11 @@ zbpc_decode_kernel(const uint8_t* __restrict__ stream, const int64_t* __restrict
     }
     const int osize = loc.osize;
     const int csize = sizes[id];
+    const uint64_t at = (uint64_t)(8 + 2 * chunks + offs[id]);
+    if (csize > osize || at + (uint64_t)csize > stream_bytes) {  // corrupt size table
+      if (tid == 0) atomicExch(error_flag, 2);
+      continue;
+    }
     const uint8_t* src = data_in + offs[id];
     uint8_t* dst = planes + loc.base;
     if (csize == osize) {  // raw chunk
@@ -408,14 +418,17 @@ zbpc_decode_kernel(const uint8_t* __restrict__ stream, const int64_t* __restrict
     __syncthreads();
     int c3 = popc_bytes_block(sh.bm3, 4, sh.scratch);
     rpos -= c3;
-    re_decode_block(sh.in + rpos, sh.bm3, 32, sh.bm2, sh.scratch);
-    int c2 = popc_bytes_block(sh.bm2, 32, sh.scratch);
+    bool ok = rpos >= 0;
+    if (ok) re_decode_block(sh.in + rpos, sh.bm3, 32, sh.bm2, sh.scratch);
+    int c2 = ok ? popc_bytes_block(sh.bm2, 32, sh.scratch) : 0;
     rpos -= c2;
-    re_decode_block(sh.in + rpos, sh.bm2, 256, sh.bm1, sh.scratch);
-    int c1 = popc_bytes_block(sh.bm1, 256, sh.scratch);
+    ok = ok && rpos >= 0;
+    if (ok) re_decode_block(sh.in + rpos, sh.bm2, 256, sh.bm1, sh.scratch);
+    int c1 = ok ? popc_bytes_block(sh.bm1, 256, sh.scratch) : 0;
     rpos -= c1;
-    re_decode_block(sh.in + rpos, sh.bm1, 2048, sh.bm0, sh.scratch);
-    if (rpos < 0) {
+    ok = ok && rpos >= 0;
+    if (ok) re_decode_block(sh.in + rpos, sh.bm1, 2048, sh.bm0, sh.scratch);
+    if (!ok) {
       if (tid == 0) atomicExch(error_flag, 2);
       __syncthreads();
       continue;

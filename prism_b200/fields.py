@@ -49,7 +49,7 @@ def grf(shape, dtype=np.float64, seed=1, slope=-5.0 / 3.0, lo=0.9, hi=3.0):
     amp = kk ** (slope / 2.0)
     amp[0, 0, 0] = 0.0
     spec = (rng.standard_normal(amp.shape) + 1j * rng.standard_normal(amp.shape)) * amp
-    f = np.fft.irfftn(spec, s=shape)
+    f = np.fft.irfftn(spec, s=shape, axes=(0, 1, 2))
     fmin, fmax = f.min(), f.max()
     f = lo + (hi - lo) * (f - fmin) / (fmax - fmin)
     return f.astype(dtype)

@@ -1,0 +1,57 @@
+"""CPU tests of the drop-in boundary: the C-ABI library loads and exports every
+entry point include/prism_b200.h declares (no compute calls without a GPU)."""
+import os
+import re
+
+import pytest
+
+import prism_b200
+from prism_b200 import _build
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    text = open(os.path.join(ROOT, "include", "prism_b200.h")).read()
+    return sorted(set(re.findall(r"\b(prism_[a-z_]+)\s*\(", text)))
+
+
+def test_library_builds_and_loads():
+    _build.build_lib()
+    assert os.path.exists(prism_b200.LIB_PATH)
+    assert prism_b200.lib() is not None
+
+
+def test_every_declared_symbol_is_exported():
+    l = prism_b200.lib()
+    syms = declared_symbols()
+    assert len(syms) >= 20
+    missing = [s for s in syms if not hasattr(l, s)]
+    assert not missing, missing
+    assert sorted(prism_b200.EXPORTED) == syms
+
+
+def test_size_queries_need_no_gpu():
+    l = prism_b200.lib()
+    # 128^3 float: host plane strides 229448/28680/3592/456 (x32)
+    assert l.prism_plane_buffer_size(128, 128, 128) == 32 * (229448 + 28680 + 3592 + 456)
+    assert l.prism_trailer_size(128, 128, 128, 4) == 1040 + 512 * 4
+    assert l.prism_max_container_size(128, 128, 128, 4) > 4 * 128 ** 3
+
+
+def test_geometry_matches_oracle():
+    import oracle as O
+    l = prism_b200.lib()
+    for dims in [(128, 128, 128), (33, 56, 64), (79, 44, 33), (100, 37, 1), (5000, 1, 1), (17, 47, 64)]:
+        g = O.geometry(*dims)
+        assert l.prism_plane_buffer_size(*dims) == g.aligned_size
+        assert l.prism_trailer_size(*dims, 8) == 1040 + g.anchors * 8
+
+
+def test_errors_are_status_codes_not_exits():
+    """Bad arguments come back as a status code (the reference exits)."""
+    import ctypes as C
+    l = prism_b200.lib()
+    size = C.c_uint64()
+    rc = l.prism_compress(None, None, 4, 1, 1, 1, 0, 1e-3, 0, None, 0, C.byref(size), None, None)
+    assert rc == -1
