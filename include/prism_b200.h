@@ -60,6 +60,18 @@ void prism_destroy(prism_handle* h);
 /* Human-readable description of the last failure on this handle. */
 const char* prism_last_error(const prism_handle* h);
 
+/* Stage timing: with profiling on, every pipeline call records CUDA events
+ * around its stages on the caller's stream (no extra synchronisation) and
+ * accumulates device milliseconds per stage.  prism_stage_times copies up to n
+ * accumulators (order: extrema, autotune, predict, shuffle, encode, trailer,
+ * strategy, decode, inverse shuffle, reconstruct), returns the stage count and
+ * clears them when reset != 0.  No counterpart in the reference, which times
+ * its stages with blocking GPUTimer pairs (include/utils/timer.hpp:21-30). */
+int prism_profile(prism_handle* h, int enable);
+int prism_stage_times(prism_handle* h, double* ms, int* counts, int n, int reset);
+/* Number of kernels this handle has launched. */
+uint64_t prism_launch_count(const prism_handle* h);
+
 /* Upper bound of the container size (all chunks stored raw). */
 uint64_t prism_max_container_size(uint32_t nx, uint32_t ny, uint32_t nz, int dtype_size);
 /* Size of the plane buffer (host aligned_size, io.cu:117-127) and the trailer. */

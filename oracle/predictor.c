@@ -5,8 +5,8 @@
 #include <string.h>
 #include "prism_oracle.h"
 
-/* Pinned contraction pattern of the reference build (filled in by the
- * parity investigation; see DESIGN.md "FP contraction"). */
+/* Pinned contraction pattern of the reference build, found by comparing the
+ * reference's codes and reconstructions with every fused variant. */
 or_fp_policy or_policy = {1, 1, 1, 1, 1, 1, 0, -1, -1, -1, -1, -1, -1, -1, -1, 2};
 void or_set_policy(const or_fp_policy* p) { or_policy = *p; }
 void or_get_policy(or_fp_policy* p) { *p = or_policy; }

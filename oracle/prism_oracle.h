@@ -57,7 +57,7 @@ typedef struct {
 void or_intp_default(or_intp* p);
 double or_alpha(double rel_eb); /* InterpolationPredictor.cu:2248-2271 */
 
-/* FP contraction policy of the reference build (see DESIGN.md).  Each knob
+/* FP contraction policy of the reference build.  Each knob
  * selects how one expression of the reference is rounded.  0 = every
  * operation rounded separately; other values = a specific fused pattern. */
 typedef struct {

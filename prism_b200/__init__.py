@@ -72,6 +72,10 @@ def lib():
         l.prism_lossless_encode.argtypes = [vp, vp, u32, u32, u32, vp, u64, C.POINTER(u64), vp, vp]
         l.prism_lossless_decode.argtypes = [vp, vp, u32, u32, u32, vp, vp, vp, vp]
         l.prism_find_strategy.argtypes = [vp, vp, dbl, dbl, vp, vp, vp, vp]
+        l.prism_profile.argtypes = [vp, i32]
+        l.prism_stage_times.argtypes = [vp, vp, vp, i32, i32]
+        l.prism_launch_count.argtypes = [vp]
+        l.prism_launch_count.restype = u64
         _lib = l
     return _lib
 
@@ -83,7 +87,11 @@ EXPORTED = [
     "prism_progressive_state", "prism_progressive_close", "prism_extrema", "prism_autotune",
     "prism_code_buffer_len", "prism_predict", "prism_reconstruct", "prism_bitshuffle",
     "prism_inverse_bitshuffle", "prism_lossless_encode", "prism_lossless_decode", "prism_find_strategy",
+    "prism_profile", "prism_stage_times", "prism_launch_count",
 ]
+
+STAGES = ["extrema", "autotune", "predict", "shuffle", "encode", "trailer", "strategy", "decode",
+          "inverse_shuffle", "reconstruct"]
 
 
 def _torch():
@@ -106,6 +114,18 @@ class Handle:
         if rc:
             msg = lib().prism_last_error(self.ptr)
             raise PrismError(f"{what}: {_STATUS.get(rc, rc)}: {msg.decode() if msg else ''}")
+
+    def profile(self, enable=True):
+        self.check(lib().prism_profile(self.ptr, int(enable)), "prism_profile")
+
+    def stage_times(self, reset=True):
+        ms = (C.c_double * 16)()
+        cnt = (C.c_int * 16)()
+        n = lib().prism_stage_times(self.ptr, ms, cnt, 16, int(reset))
+        return {STAGES[i]: (ms[i], cnt[i]) for i in range(min(n, len(STAGES)))}
+
+    def launches(self):
+        return int(lib().prism_launch_count(self.ptr))
 
     def close(self):
         if self.ptr:

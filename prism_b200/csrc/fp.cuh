@@ -1,7 +1,8 @@
 // Explicitly rounded arithmetic.  The predictor must reproduce the reference
 // build's rounding bit for bit, so every add/mul/fma below is an intrinsic the
 // compiler may not re-contract or re-associate.  The contraction pattern is the
-// one measured against the reference build on a B200.
+// one measured against the reference build on a B200: every expression was
+// compared in all its fused variants and the matching one kept.
 #pragma once
 #include <cuda_runtime.h>
 

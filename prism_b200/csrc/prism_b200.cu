@@ -72,12 +72,44 @@ struct HostResult {
 
 }  // namespace
 
+// pipeline stages timed when profiling is on (prism_profile)
+enum Stage { kStExtrema, kStAutotune, kStPredict, kStShuffle, kStEncode, kStTrailer, kStStrategy, kStDecode,
+             kStInverse, kStReconstruct, kStCount };
+
 struct prism_handle {
   DevBuf qc, planes, status, offs, bsum, part, wins, ranges, anchors, small, dev_in, dev_out, zero_anchors;
   HostResult* host = nullptr;  // pinned
   std::string err;
   int sm_count = 148;
+  uint64_t launches = 0;       // kernels launched by this handle
+  bool prof = false;
+  cudaEvent_t ev[kStCount][2] = {};
+  bool pending[kStCount] = {};
+  double acc_ms[kStCount] = {};
+  int acc_n[kStCount] = {};
 };
+
+static void prof_begin(prism_handle* h, int stage, cudaStream_t st) {
+  if (h->prof) cudaEventRecord(h->ev[stage][0], st);
+}
+static void prof_end(prism_handle* h, int stage, cudaStream_t st) {
+  if (h->prof) {
+    cudaEventRecord(h->ev[stage][1], st);
+    h->pending[stage] = true;
+  }
+}
+// after a stream sync: fold the recorded stage times into the accumulators
+static void prof_collect(prism_handle* h) {
+  for (int i = 0; i < kStCount; ++i) {
+    if (!h->pending[i]) continue;
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, h->ev[i][0], h->ev[i][1]) == cudaSuccess) {
+      h->acc_ms[i] += ms;
+      h->acc_n[i] += 1;
+    }
+    h->pending[i] = false;
+  }
+}
 
 struct prism_prog {
   prism_handle* h;
@@ -149,8 +181,11 @@ template <class T>
 static int launch_extrema(prism_handle* h, const T* in, uint64_t n, cudaStream_t st) {
   int blocks = (int)std::min<uint64_t>((n + kExtThreads - 1) / kExtThreads, (uint64_t)h->sm_count * 4);
   CKA(h->part.ensure(sizeof(T) * 2 * blocks));
+  prof_begin(h, kStExtrema, st);
   extrema_kernel<T><<<blocks, kExtThreads, 0, st>>>(in, n, h->part.as<T>());
   extrema_final_kernel<T><<<1, 32, 0, st>>>(h->part.as<T>(), blocks, &small(h)->range);
+  prof_end(h, kStExtrema, st);
+  h->launches += 2;
   CK(cudaGetLastError());
   return PRISM_OK;
 }
@@ -180,11 +215,15 @@ static int launch_autotune_params(prism_handle* h, const T* in, const Geometry& 
     if (nwin > 0) {
       CKA(h->wins.ensure(sizeof(SampleWindow) * nwin));
       CK(cudaMemcpyAsync(h->wins.p, wins.data(), sizeof(SampleWindow) * nwin, cudaMemcpyHostToDevice, st));
+      prof_begin(h, kStAutotune, st);
       autotune_kernel<T><<<dim3(nwin, 6), kAttThreads, 0, st>>>(in, g, h->wins.as<SampleWindow>(), h->part.as<T>());
+      prof_end(h, kStAutotune, st);
+      h->launches += 1;
     }
     params_kernel<T><<<1, 32, 0, st>>>(mode, bound, &s->range, alpha, h->part.as<T>(), nwin, nullptr, 4,
                                        reinterpret_cast<PredParams<T>*>(s->params),
                                        reinterpret_cast<T*>(s->errors), &s->eb);
+    h->launches += 1;
   } else {
     params_kernel<T><<<1, 32, 0, st>>>(mode, bound, &s->range, alpha, nullptr, 0, force_flags_dev, 4,
                                        reinterpret_cast<PredParams<T>*>(s->params), nullptr, &s->eb);
@@ -224,10 +263,12 @@ static int launch_bitshuffle(prism_handle* h, const int32_t* qc, const Geometry&
   ShufPlan plan = make_shuf_plan(g, start_last);
   ByteRange rng[160];
   int nr = fill_ranges(g, plan, rng, 160);
+  prof_begin(h, kStShuffle, st);
   if (nr > 0) {
     CKA(h->ranges.ensure(sizeof(rng)));
     CK(cudaMemcpyAsync(h->ranges.p, rng, sizeof(ByteRange) * nr, cudaMemcpyHostToDevice, st));
     leftover_fill_kernel<<<nr, 256, 0, st>>>(planes, qc, g, h->ranges.as<ByteRange>(), nr);
+    h->launches += 1;
   }
   const int32_t* codes = qc + g.anchors;
   bool last_last = last_block_lands_last(g);
@@ -237,6 +278,8 @@ static int launch_bitshuffle(prism_handle* h, const int32_t* qc, const Geometry&
     bitshuffle_kernel<<<(unsigned)blocks, kShufWarps * 32, 0, st>>>(codes, planes, g, plan, nb);
   }
   if (last_last) shuffle_last_block_kernel<<<1, 512, 0, st>>>(codes, planes, g, nb, g.aligned_size);
+  prof_end(h, kStShuffle, st);
+  h->launches += 1 + (plan.items > 0);
   CK(cudaGetLastError());
   return PRISM_OK;
 }
@@ -250,11 +293,15 @@ static int launch_inverse(prism_handle* h, const uint8_t* planes, const Geometry
   if (to > from) CK(cudaMemsetAsync(qc + from, 0, (to - from) * sizeof(int32_t), st));
   ShufPlan plan = make_shuf_plan(g, start_last);
   int32_t* codes = qc + g.anchors;
+  prof_begin(h, kStInverse, st);
   if (plan.items > 0) {
     int64_t blocks = (plan.items + kShufWarps - 1) / kShufWarps;
     inverse_bitshuffle_kernel<<<(unsigned)blocks, kShufWarps * 32, 0, st>>>(planes, codes, g, plan, nb, dbegin, dend);
+    h->launches += 1;
   }
   inverse_last_block_kernel<<<1, 512, 0, st>>>(planes, codes, g, nb, dbegin, dend, g.aligned_size);
+  prof_end(h, kStInverse, st);
+  h->launches += 1;
   CK(cudaGetLastError());
   return PRISM_OK;
 }
@@ -272,10 +319,13 @@ static int launch_encode(prism_handle* h, const uint8_t* planes, const Geometry&
     attr_set = true;
   }
   int blocks = (int)std::min<int64_t>(g.chunks, (int64_t)h->sm_count * 4);
+  prof_begin(h, kStEncode, st);
   zbpc_encode_kernel<<<blocks, kZThreads, smem, st>>>(planes, g, stream, h->status.as<unsigned long long>(),
                                                       &s->ticket, s->csbp, &s->lossless_size, &s->error_flag,
                                                       (long long)1 << 22);
   zbpc_finish_kernel<<<1, 32, 0, st>>>(stream, g, &s->lossless_size, &s->padded_size);
+  prof_end(h, kStEncode, st);
+  h->launches += 2;
   CK(cudaGetLastError());
   return PRISM_OK;
 }
@@ -285,6 +335,7 @@ static int launch_decode(prism_handle* h, const uint8_t* stream, uint64_t stream
   Small* s = small(h);
   const uint16_t* sizes = reinterpret_cast<const uint16_t*>(stream + 8);
   int64_t nblk = (g.chunks + kScanItems - 1) / kScanItems;
+  prof_begin(h, kStDecode, st);
   scan_sizes_block<<<(unsigned)nblk, 1024, 0, st>>>(sizes, g.chunks, h->offs.as<int64_t>(), h->bsum.as<int64_t>());
   scan_block_sums<<<1, 32, 0, st>>>(h->bsum.as<int64_t>(), nblk);
   scan_add<<<(unsigned)((g.chunks + 255) / 256), 256, 0, st>>>(h->offs.as<int64_t>(), g.chunks, h->bsum.as<int64_t>());
@@ -298,6 +349,8 @@ static int launch_decode(prism_handle* h, const uint8_t* stream, uint64_t stream
   int blocks = (int)std::min<int64_t>(g.chunks, (int64_t)h->sm_count * 8);
   zbpc_decode_kernel<<<blocks, kZThreads, smem, st>>>(stream, stream_bytes, h->offs.as<int64_t>(), g, planes,
                                                       dbegin, dend, &s->error_flag);
+  prof_end(h, kStDecode, st);
+  h->launches += 4;
   CK(cudaGetLastError());
   return PRISM_OK;
 }
@@ -327,6 +380,7 @@ static int finish(prism_handle* h, cudaStream_t st) {
   CK(cudaMemcpyAsync(h->host->params, s->params, sizeof(s->params), cudaMemcpyDeviceToHost, st));
   CK(cudaMemcpyAsync(h->host->errors, s->errors, sizeof(s->errors), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
+  prof_collect(h);
   if (h->host->error_flag == 1) return fail(h, PRISM_ERR_TIMEOUT, "look-back wait exceeded its limit");
   if (h->host->error_flag == 2) return fail(h, PRISM_ERR_CORRUPT, "corrupt lossless chunk");
   return PRISM_OK;
@@ -350,15 +404,21 @@ static int compress_t(prism_handle* h, const T* in, const Geometry& g, int mode,
   if (rc) return rc;
   rc = zero_code_padding(h, g, st);
   if (rc) return rc;
+  prof_begin(h, kStPredict, st);
   predict_compress_kernel<T><<<(unsigned)g.anchors, kPredThreads, 0, st>>>(in, g, params_ptr<T>(h), h->anchors.as<T>(),
                                                                             h->qc.as<int32_t>());
+  prof_end(h, kStPredict, st);
+  h->launches += 1;
   CK(cudaGetLastError());
   rc = launch_bitshuffle(h, h->qc.as<int32_t>(), g, nb, h->planes.as<uint8_t>(), st);
   if (rc) return rc;
   rc = launch_encode(h, h->planes.as<uint8_t>(), g, out, st);
   if (rc) return rc;
+  prof_begin(h, kStTrailer, st);
   trailer_kernel<T><<<64, 256, 0, st>>>(out, &s->padded_size, params_ptr<T>(h), &s->range, s->csbp,
                                         h->anchors.as<T>(), g.anchors);
+  prof_end(h, kStTrailer, st);
+  h->launches += 1;
   CK(cudaGetLastError());
   rc = finish(h, st);
   if (rc) return rc;
@@ -385,8 +445,11 @@ static int decompress_t(prism_handle* h, const uint8_t* cont, uint64_t size, con
   if (rc) return rc;
   rc = launch_inverse(h, h->planes.as<uint8_t>(), g, 0 /*SM*/, nullptr, nullptr, h->qc.as<int32_t>(), st);
   if (rc) return rc;
+  prof_begin(h, kStReconstruct, st);
   reconstruct_kernel<T, false><<<(unsigned)g.anchors, kPredThreads, 0, st>>>(
       h->qc.as<int32_t>(), reinterpret_cast<const T*>(tr + 1040), g, params_ptr<T>(h), nullptr, out);
+  prof_end(h, kStReconstruct, st);
+  h->launches += 2;
   CK(cudaGetLastError());
   return finish(h, st);
 }
@@ -414,11 +477,38 @@ void prism_destroy(prism_handle* h) {
   DevBuf* bufs[] = {&h->qc, &h->planes, &h->status, &h->offs, &h->bsum, &h->part, &h->wins, &h->ranges,
                     &h->anchors, &h->small, &h->dev_in, &h->dev_out, &h->zero_anchors};
   for (DevBuf* b : bufs) b->release();
+  for (int i = 0; i < kStCount; ++i)
+    for (int j = 0; j < 2; ++j)
+      if (h->ev[i][j]) cudaEventDestroy(h->ev[i][j]);
   if (h->host) cudaFreeHost(h->host);
   delete h;
 }
 
 const char* prism_last_error(const prism_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+int prism_profile(prism_handle* h, int enable) {
+  if (!h) return PRISM_ERR_ARG;
+  if (enable && !h->ev[0][0]) {
+    for (int i = 0; i < kStCount; ++i)
+      for (int j = 0; j < 2; ++j)
+        if (cudaEventCreate(&h->ev[i][j]) != cudaSuccess) return fail(h, PRISM_ERR_CUDA, "cudaEventCreate");
+  }
+  h->prof = enable != 0;
+  return PRISM_OK;
+}
+
+int prism_stage_times(prism_handle* h, double* ms, int* counts, int n, int reset) {
+  if (!h || !ms) return PRISM_ERR_ARG;
+  for (int i = 0; i < n && i < kStCount; ++i) {
+    ms[i] = h->acc_ms[i];
+    if (counts) counts[i] = h->acc_n[i];
+  }
+  if (reset)
+    for (int i = 0; i < kStCount; ++i) { h->acc_ms[i] = 0; h->acc_n[i] = 0; }
+  return kStCount;
+}
+
+uint64_t prism_launch_count(const prism_handle* h) { return h ? h->launches : 0; }
 
 uint64_t prism_max_container_size(uint32_t nx, uint32_t ny, uint32_t nz, int dtype_size) {
   Geometry g;
@@ -550,8 +640,11 @@ static int progressive_step_t(prism_prog* p, double target, T* values, cudaStrea
   CK(cudaMemcpyAsync(&s->sstate, &p->state, sizeof(StrategyState), cudaMemcpyHostToDevice, st));
   // strategy (findStrategy_h) from the container's cumulative plane sizes
   const uint64_t* csbp = reinterpret_cast<const uint64_t*>(tr + 16);
+  prof_begin(h, kStStrategy, st);
   strategy_search_kernel<<<33, 1024, 0, st>>>(csbp, p->mode, p->bound, target, &s->range, s->sblk);
   strategy_finish_kernel<<<1, 32, 0, st>>>(s->sblk, p->mode, p->bound, target, &s->range, &s->sstate);
+  prof_end(h, kStStrategy, st);
+  h->launches += 3;
   // parameters with maxlevel from the strategy
   params_kernel<T><<<1, 32, 0, st>>>(p->mode, p->bound, &s->range, alpha_of(p->mode == 1 ? p->bound : 0.0), nullptr,
                                      0, tr, 4, reinterpret_cast<PredParams<T>*>(s->params), nullptr, &s->eb);
@@ -563,6 +656,7 @@ static int progressive_step_t(prism_prog* p, double target, T* values, cudaStrea
   if (rc) return rc;
   rc = launch_inverse(h, h->planes.as<uint8_t>(), g, 1 /*NB*/, s->sstate.begin, s->sstate.end, h->qc.as<int32_t>(), st);
   if (rc) return rc;
+  prof_begin(h, kStReconstruct, st);
   if (first) {
     reconstruct_kernel<T, false><<<(unsigned)g.anchors, kPredThreads, 0, st>>>(
         h->qc.as<int32_t>(), reinterpret_cast<const T*>(tr + 1040), g, params_ptr<T>(h), nullptr, values);
@@ -571,6 +665,8 @@ static int progressive_step_t(prism_prog* p, double target, T* values, cudaStrea
     reconstruct_kernel<T, true><<<(unsigned)g.anchors, kPredThreads, 0, st>>>(
         h->qc.as<int32_t>(), h->zero_anchors.as<T>(), g, params_ptr<T>(h), values, values);
   }
+  prof_end(h, kStReconstruct, st);
+  h->launches += 1;
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(&p->state, &s->sstate, sizeof(StrategyState), cudaMemcpyDeviceToHost, st));
   rc = finish(h, st);

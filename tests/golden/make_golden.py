@@ -16,7 +16,9 @@ buffers raw (gzip) and reduces large ones to SHA-256 digests, then writes
 
 ``cases.json`` (next to this file) lists the cases.  Run:
 
-    python tests/golden/make_golden.py --out gpurun_out/golden [--big]
+    python tests/golden/make_golden.py --out <dir> [--big]
+
+and copy the case folders into ``tests/golden/``.
 """
 from __future__ import annotations
 
@@ -126,7 +128,7 @@ def run_cli(case, out_root, prism, tmp, tag):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden"))
+    ap.add_argument("--out", required=True, help="output folder for the case dumps")
     ap.add_argument("--cases", default=os.path.join(HERE, "cases.json"))
     ap.add_argument("--only", default="")
     ap.add_argument("--big", action="store_true", help="also run the large configurations")
