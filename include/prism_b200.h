@@ -48,7 +48,8 @@ enum prism_status {
   PRISM_ERR_CUDA = -2,       /* CUDA runtime error */
   PRISM_ERR_CORRUPT = -3,    /* container does not parse / decode */
   PRISM_ERR_TIMEOUT = -4,    /* a device-side wait hit its iteration limit */
-  PRISM_ERR_NOMEM = -5       /* device workspace allocation failed */
+  PRISM_ERR_NOMEM = -5,      /* device workspace allocation failed */
+  PRISM_ERR_LIMIT = -6       /* input larger than a fixed-size entry point accepts */
 };
 
 typedef struct prism_handle prism_handle;
@@ -149,6 +150,34 @@ int prism_lossless_encode(prism_handle* h, const uint8_t* d_planes, uint32_t nx,
 int prism_lossless_decode(prism_handle* h, const uint8_t* d_stream, uint32_t nx, uint32_t ny,
                           uint32_t nz, const int begin[4], const int end[4], uint8_t* d_planes,
                           void* stream);
+/* Lossless encode that allocates nothing.  No counterpart in the reference.
+ *
+ * Same result as prism_lossless_encode (bit-identical stream, size and plane
+ * sizes) without a handle: its scratch (look-back status words, chunk ticket,
+ * error flag, plane sizes; about 130 KiB) is a fixed device array inside the
+ * library, so neither this call nor anything it calls allocates device or host
+ * memory.  Meant for callers that cannot allocate at this point, e.g. a process
+ * whose device memory is fully reserved by another allocator, or a
+ * latency-critical loop in which cudaMalloc/cudaFree would synchronise the
+ * device and stall the work on other streams.
+ *
+ * Limit: at most 16384 lossless chunks, i.e. a plane buffer
+ * (prism_plane_buffer_size) of at most 256 MiB, about 64 million values;
+ * larger fields return PRISM_ERR_LIMIT before any device work.
+ * Zero state: the call itself resets, on `stream`, every scratch word the
+ * kernels expect to start at zero; the caller zeroes nothing.
+ * Overlap: there is one scratch per device for the whole process, so two calls
+ * whose device work may overlap (different streams, different host threads)
+ * race on it and produce wrong output; order them on one stream or with
+ * events.  The call waits for its stream before it returns.
+ * Setup: the first call on each device (with that device current) looks up
+ * the scratch address and sets the encode kernel's shared-memory limit; make
+ * that first call before any stream capture begins.
+ * Other errors: PRISM_ERR_ARG for bad arguments or capacity, PRISM_ERR_CUDA,
+ * PRISM_ERR_TIMEOUT as for prism_lossless_encode. */
+int prism_lossless_encode_static(const uint8_t* d_planes, uint32_t nx, uint32_t ny, uint32_t nz,
+                                 uint8_t* d_stream, uint64_t capacity, uint64_t* size_out,
+                                 uint64_t comp_size_bp[128], void* stream);
 /* Strategy step: updates begin/end/maxlevel (host arrays) from the cumulative
  * plane sizes (host), the absolute bound and the absolute target error. */
 int prism_find_strategy(prism_handle* h, const uint64_t comp_size_bp[128], double eb,

@@ -27,7 +27,8 @@ ABS, REL = 0, 1
 SM, NB = 0, 1  # progressive=0 -> sign-magnitude planes, 1 -> negabinary
 
 _STATUS = {0: "ok", -1: "bad argument", -2: "CUDA error", -3: "corrupt container",
-           -4: "device wait timed out", -5: "out of device memory"}
+           -4: "device wait timed out", -5: "out of device memory",
+           -6: "input larger than the entry point's fixed limit"}
 
 
 class PrismError(RuntimeError):
@@ -72,6 +73,7 @@ def lib():
         l.prism_lossless_encode.argtypes = [vp, vp, u32, u32, u32, vp, u64, C.POINTER(u64), vp, vp]
         l.prism_lossless_decode.argtypes = [vp, vp, u32, u32, u32, vp, vp, vp, vp]
         l.prism_find_strategy.argtypes = [vp, vp, dbl, dbl, vp, vp, vp, vp]
+        l.prism_lossless_encode_static.argtypes = [vp, u32, u32, u32, vp, u64, C.POINTER(u64), vp, vp]
         l.prism_profile.argtypes = [vp, i32]
         l.prism_stage_times.argtypes = [vp, vp, vp, i32, i32]
         l.prism_launch_count.argtypes = [vp]
@@ -87,7 +89,7 @@ EXPORTED = [
     "prism_progressive_state", "prism_progressive_close", "prism_extrema", "prism_autotune",
     "prism_code_buffer_len", "prism_predict", "prism_reconstruct", "prism_bitshuffle",
     "prism_inverse_bitshuffle", "prism_lossless_encode", "prism_lossless_decode", "prism_find_strategy",
-    "prism_profile", "prism_stage_times", "prism_launch_count",
+    "prism_profile", "prism_stage_times", "prism_launch_count", "prism_lossless_encode_static",
 ]
 
 STAGES = ["extrema", "autotune", "predict", "shuffle", "encode", "trailer", "strategy", "decode",

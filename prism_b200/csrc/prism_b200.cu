@@ -6,9 +6,11 @@
 // block at the end of a call.  Device workspace is cached in the handle and
 // only grows.
 #include <cuda_runtime.h>
+#include <stddef.h>
 #include <stdio.h>
 #include <string.h>
 #include <algorithm>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -899,3 +901,106 @@ int prism_find_strategy(prism_handle* h, const uint64_t comp_size_bp[128], doubl
   return PRISM_OK;
 }
 
+
+// ---------------------------------------------------------------------------
+// Lossless encode without any allocation (prism_lossless_encode_static).
+//
+// Same kernels as prism_lossless_encode, but the look-back status words, the
+// chunk ticket, the error flag and the small results live in one file-scope
+// device array instead of a handle's workspace, so the call allocates nothing.
+// The array is shared by every call in the process on a given device: calls
+// whose device work overlaps (different streams, different host threads) race
+// on it and must be ordered by the caller.
+namespace {
+
+constexpr int64_t kStaticMaxChunks = 16384;  // plane buffer <= 256 MiB
+
+struct StaticEncodeScratch {
+  unsigned long long status[kStaticMaxChunks];  // zeroed by every call
+  unsigned long long ticket;                    // zeroed by every call
+  int error_flag;                               // zeroed by every call
+  int pad;
+  uint64_t csbp[128];                           // zeroed by every call
+  uint64_t lossless_size;
+  uint64_t padded_size;
+};
+
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_static_encode_scratch[sizeof(StaticEncodeScratch)];
+
+namespace {
+
+constexpr int kStaticMaxDevices = 64;
+
+struct StaticEncodeSetup {
+  bool ready = false;
+  StaticEncodeScratch* scratch = nullptr;
+  int sm_count = 0;
+};
+
+std::mutex g_static_setup_mutex;
+StaticEncodeSetup g_static_setup[kStaticMaxDevices];
+
+// Once per device, with that device current: look up the scratch address,
+// raise the encode kernel's dynamic shared-memory limit and read the SM count.
+int static_encode_setup(int dev, StaticEncodeSetup* out) {
+  std::lock_guard<std::mutex> lock(g_static_setup_mutex);
+  StaticEncodeSetup& s = g_static_setup[dev];
+  if (!s.ready) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_static_encode_scratch) != cudaSuccess) return PRISM_ERR_CUDA;
+    if (cudaFuncSetAttribute(zbpc_encode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(EncodeShared)) != cudaSuccess)
+      return PRISM_ERR_CUDA;
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return PRISM_ERR_CUDA;
+    s.scratch = static_cast<StaticEncodeScratch*>(p);
+    s.sm_count = sms;
+    s.ready = true;
+  }
+  *out = s;
+  return PRISM_OK;
+}
+
+}  // namespace
+
+int prism_lossless_encode_static(const uint8_t* d_planes, uint32_t nx, uint32_t ny, uint32_t nz,
+                                 uint8_t* d_stream, uint64_t capacity, uint64_t* size_out,
+                                 uint64_t comp_size_bp[128], void* stream) {
+  if (!d_planes || !d_stream || !size_out || !dims_ok(nx, ny, nz)) return PRISM_ERR_ARG;
+  Geometry g;
+  make_geometry(nx, ny, nz, 4, &g);
+  if (g.chunks > kStaticMaxChunks) return PRISM_ERR_LIMIT;
+  if (capacity < 8 + 2 * (uint64_t)g.chunks + g.aligned_size + 8) return PRISM_ERR_ARG;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return PRISM_ERR_CUDA;
+  if (dev < 0 || dev >= kStaticMaxDevices) return PRISM_ERR_ARG;
+  StaticEncodeSetup setup;
+  int rc = static_encode_setup(dev, &setup);
+  if (rc) return rc;
+  StaticEncodeScratch* s = setup.scratch;
+  cudaStream_t st = (cudaStream_t)stream;
+  // everything the encode kernel expects at zero, reset on the caller's stream
+  if (cudaMemsetAsync(s->status, 0, (size_t)g.chunks * sizeof(unsigned long long), st) != cudaSuccess ||
+      cudaMemsetAsync(&s->ticket, 0,
+                      offsetof(StaticEncodeScratch, lossless_size) - offsetof(StaticEncodeScratch, ticket),
+                      st) != cudaSuccess)
+    return PRISM_ERR_CUDA;
+  int blocks = (int)std::min<int64_t>(g.chunks, (int64_t)setup.sm_count * 4);
+  zbpc_encode_kernel<<<blocks, kZThreads, sizeof(EncodeShared), st>>>(
+      d_planes, g, d_stream, s->status, &s->ticket, s->csbp, &s->lossless_size, &s->error_flag, (long long)1 << 22);
+  zbpc_finish_kernel<<<1, 32, 0, st>>>(d_stream, g, &s->lossless_size, &s->padded_size);
+  if (cudaGetLastError() != cudaSuccess) return PRISM_ERR_CUDA;
+  uint64_t padded = 0;
+  int flag = 0;
+  if (cudaMemcpyAsync(&padded, &s->padded_size, sizeof(padded), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+      cudaMemcpyAsync(&flag, &s->error_flag, sizeof(flag), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    return PRISM_ERR_CUDA;
+  if (comp_size_bp && cudaMemcpyAsync(comp_size_bp, s->csbp, 1024, cudaMemcpyDeviceToHost, st) != cudaSuccess)
+    return PRISM_ERR_CUDA;
+  if (cudaStreamSynchronize(st) != cudaSuccess) return PRISM_ERR_CUDA;
+  if (flag == 1) return PRISM_ERR_TIMEOUT;
+  *size_out = padded;
+  return PRISM_OK;
+}
