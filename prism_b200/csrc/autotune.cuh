@@ -150,7 +150,7 @@ autotune_kernel(const T* __restrict__ data, Geometry g, const SampleWindow* __re
   t.s = win;
   t.dim[0] = g.nx; t.dim[1] = g.ny; t.dim[2] = g.nz;
 #pragma unroll
-  for (int d = 0; d < 3; ++d) { t.gs[d] = w.gs[d]; t.notlast[d] = w.gs[d] + 16u < t.dim[d]; }
+  for (int d = 0; d < 3; ++d) { t.gs[d] = w.gs[d]; t.notlast_[d] = w.gs[d] + 16u < t.dim[d]; }
   const uint64_t sy = g.nx, sz = (uint64_t)g.nx * g.ny;
   for (int i = threadIdx.x; i < kWinVol; i += blockDim.x) {
     int x = i % kWin, y = (i / kWin) % kWin, z = i / (kWin * kWin);
@@ -254,7 +254,19 @@ __global__ void __launch_bounds__(kExtThreads)
 extrema_kernel(const T* __restrict__ in, uint64_t n, T* __restrict__ part) {
   __shared__ T smin[kExtThreads], smax[kExtThreads];
   T mn = in[0], mx = in[0];
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (; i + 3 * stride < n; i += 4 * stride) {  // four independent loads in flight
+    T v[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) v[k] = __ldg(in + i + k * stride);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      mn = v[k] < mn ? v[k] : mn;
+      mx = v[k] > mx ? v[k] : mx;
+    }
+  }
+  for (; i < n; i += stride) {
     T v = __ldg(in + i);
     mn = v < mn ? v : mn;
     mx = v > mx ? v : mx;
@@ -273,16 +285,23 @@ extrema_kernel(const T* __restrict__ in, uint64_t n, T* __restrict__ part) {
   if (threadIdx.x == 0) { part[2 * blockIdx.x] = smin[0]; part[2 * blockIdx.x + 1] = smax[0]; }
 }
 
+// one warp folds the per-block extrema (min/max are order independent)
 template <class T>
 __global__ void extrema_final_kernel(const T* __restrict__ part, int nblocks, double* __restrict__ range) {
-  if (threadIdx.x != 0) return;
+  const int lane = threadIdx.x;
   T mn = part[0], mx = part[1];
-  for (int b = 1; b < nblocks; ++b) {
+  for (int b = lane; b < nblocks; b += 32) {
     T a = part[2 * b], c = part[2 * b + 1];
     mn = a < mn ? a : mn;
     mx = c > mx ? c : mx;
   }
-  *range = __dsub_rn((double)mx, (double)mn);
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) {
+    T a = __shfl_xor_sync(0xffffffffu, mn, d), c = __shfl_xor_sync(0xffffffffu, mx, d);
+    mn = a < mn ? a : mn;
+    mx = c > mx ? c : mx;
+  }
+  if (lane == 0) *range = __dsub_rn((double)mx, (double)mn);
 }
 
 }  // namespace prism_b200

@@ -19,8 +19,8 @@
 
 namespace prism_b200 {
 
-constexpr int kShufWarps = 8;  // warps per CTA
-constexpr int kShufCodes = 256;  // codes per warp work item
+constexpr int kShufWarps = 8;     // warps per CTA
+constexpr int kShufCodes = 1024;  // codes per warp work item (128 bytes per plane)
 
 __device__ __forceinline__ uint32_t warp_transpose32(uint32_t x, int lane) {
   const uint32_t masks[5] = {0x0000FFFFu, 0x00FF00FFu, 0x0F0F0F0Fu, 0x33333333u, 0x55555555u};
@@ -49,7 +49,13 @@ __device__ __forceinline__ int32_t sign_inverse(uint32_t a, bool nb) {
 __device__ __forceinline__ uint32_t to_plane_bytes(uint32_t w) { return __byte_perm(__brev(w), 0, 0x0123); }
 __device__ __forceinline__ uint32_t from_plane_bytes(uint32_t b) { return __brev(__byte_perm(b, 0, 0x0123)); }
 
-// Work decomposition: per level a run of 256-code items.
+// a[i] of a 4-entry array held in kernel parameters, without the local-memory
+// copy a dynamic index would force
+__device__ __forceinline__ int64_t pick4(const int64_t (&a)[4], int i) {
+  return i == 0 ? a[0] : (i == 1 ? a[1] : (i == 2 ? a[2] : a[3]));
+}
+
+// Work decomposition: per level a run of kShufCodes-code items.
 struct ShufPlan {
   int64_t seg_start[4];   // device code index where the level starts
   int64_t proc[4];        // codes of the level that get real planes
@@ -77,87 +83,106 @@ inline ShufPlan make_shuf_plan(const Geometry& g, int64_t limit) {
 
 __device__ __forceinline__ void locate_item(const ShufPlan& s, int64_t item, int* level, int64_t* local) {
   int k = 0;
-  while (k < 3 && item >= s.item_prefix[k + 1]) ++k;
+  if (item >= s.item_prefix[1]) k = 1;
+  if (item >= s.item_prefix[2]) k = 2;
+  if (item >= s.item_prefix[3]) k = 3;
   *level = 3 - k;
-  *local = item - s.item_prefix[k];
+  *local = item - (k == 0 ? s.item_prefix[0] : (k == 1 ? s.item_prefix[1] : (k == 2 ? s.item_prefix[2] : s.item_prefix[3])));
 }
 
-// codes (qc + anchors, device code space) -> planes
+// codes (qc + anchors, device code space) -> planes.  A warp takes 1024
+// consecutive codes of one level: 32 coalesced 128-byte loads, 32 register
+// transposes, then through a padded shared-memory tile so that each plane's
+// 128 bytes leave as one contiguous warp store.
 __global__ void __launch_bounds__(kShufWarps * 32)
 bitshuffle_kernel(const int32_t* __restrict__ codes, uint8_t* __restrict__ planes, Geometry g,
                   ShufPlan plan, int nb) {
-  const int lane = threadIdx.x & 31;
-  int64_t item = (int64_t)blockIdx.x * kShufWarps + (threadIdx.x >> 5);
+  __shared__ uint32_t tile[kShufWarps][32][33];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int64_t item = (int64_t)blockIdx.x * kShufWarps + warp;
   if (item >= plan.items) return;
   int level;
   int64_t local;
   locate_item(plan, item, &level, &local);
-  int64_t first = local * kShufCodes;  // within the level
-  int64_t count = plan.proc[level] - first;
+  const int64_t first = local * kShufCodes;  // within the level
+  int64_t count = pick4(plan.proc, level) - first;
   if (count > kShufCodes) count = kShufCodes;
-  const int32_t* src = codes + plan.seg_start[level] + first;
-  uint32_t words[8];
+  const int32_t* src = codes + pick4(plan.seg_start, level) + first;
+  uint32_t (&tw)[32][33] = tile[warp];
+  if (count == kShufCodes) {
+    int32_t c[32];
 #pragma unroll
-  for (int it = 0; it < 8; ++it) {
-    int idx = it * 32 + lane;
-    int32_t c = idx < count ? __ldg(src + idx) : 0;
-    uint32_t w = sign_transform(c, nb);
-    words[it] = to_plane_bytes(warp_transpose32(w, lane));
-  }
-  // lane i holds plane 31 - i
-  int p = 31 - lane;
-  uint8_t* dst = planes + g.daprefix[level] + (int64_t)p * g.dstride[level] + first / 8;
-  int nbytes = (int)(count / 8);
-  if (nbytes == 32) {
-    uint2* d2 = reinterpret_cast<uint2*>(dst);
+    for (int it = 0; it < 32; ++it) c[it] = __ldg(src + it * 32 + lane);
 #pragma unroll
-    for (int q = 0; q < 4; ++q) d2[q] = make_uint2(words[2 * q], words[2 * q + 1]);
+    for (int it = 0; it < 32; ++it) tw[lane][it] = to_plane_bytes(warp_transpose32(sign_transform(c[it], nb), lane));
   } else {
-    for (int b = 0; b < nbytes; ++b) dst[b] = (uint8_t)(words[b >> 2] >> (8 * (b & 3)));
+#pragma unroll 4
+    for (int it = 0; it < 32; ++it) {
+      int idx = it * 32 + lane;
+      int32_t c = idx < count ? __ldg(src + idx) : 0;
+      tw[lane][it] = to_plane_bytes(warp_transpose32(sign_transform(c, nb), lane));
+    }
+  }
+  __syncwarp();
+  // row r holds plane 31 - r; word j = plane bytes 4j..4j+3 of this item
+  const int nbytes = (int)(count / 8);
+  const int64_t stride = pick4(g.dstride, level);
+  uint8_t* base = planes + pick4(g.daprefix, level) + first / 8;
+#pragma unroll 4
+  for (int r = 0; r < 32; ++r) {
+    uint8_t* dst = base + (int64_t)(31 - r) * stride;
+    uint32_t w = tw[r][lane];
+    if (4 * lane + 4 <= nbytes) {
+      reinterpret_cast<uint32_t*>(dst)[lane] = w;
+    } else if (4 * lane < nbytes) {
+      for (int b = 4 * lane; b < nbytes; ++b) dst[b] = (uint8_t)(w >> (8 * (b & 3)));
+    }
   }
 }
 
 // planes -> codes; begin/end (device, may be null) restrict each level to
-// planes [begin[3-l], end[3-l]) exactly as the progressive inverse does
+// planes [begin[3-l], end[3-l]) exactly as the progressive inverse does.
+// Rows of planes outside that range are never read.
 __global__ void __launch_bounds__(kShufWarps * 32)
 inverse_bitshuffle_kernel(const uint8_t* __restrict__ planes, int32_t* __restrict__ codes, Geometry g,
                           ShufPlan plan, int nb, const int* __restrict__ begin, const int* __restrict__ end) {
-  const int lane = threadIdx.x & 31;
-  int64_t item = (int64_t)blockIdx.x * kShufWarps + (threadIdx.x >> 5);
+  __shared__ uint32_t tile[kShufWarps][32][33];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int64_t item = (int64_t)blockIdx.x * kShufWarps + warp;
   if (item >= plan.items) return;
   int level;
   int64_t local;
   locate_item(plan, item, &level, &local);
-  int64_t first = local * kShufCodes;
-  int64_t count = plan.proc[level] - first;
+  const int64_t first = local * kShufCodes;
+  int64_t count = pick4(plan.proc, level) - first;
   if (count > kShufCodes) count = kShufCodes;
-  int p = 31 - lane;
-  bool take = true;
-  if (begin) {
-    int lo = begin[3 - level], hi = end[3 - level];
-    take = lo < hi && p >= lo && p < hi;
-  }
-  const uint8_t* src = planes + g.daprefix[level] + (int64_t)p * g.dstride[level] + first / 8;
-  int nbytes = (int)(count / 8);
-  uint32_t words[8];
-  if (take && nbytes == 32) {
-    const uint2* s2 = reinterpret_cast<const uint2*>(src);
+  int lo = 0, hi = 32;
+  if (begin) { lo = begin[3 - level]; hi = end[3 - level]; }
+  const int nbytes = (int)(count / 8);
+  const int64_t stride = pick4(g.dstride, level);
+  const uint8_t* base = planes + pick4(g.daprefix, level) + first / 8;
+  uint32_t (&tw)[32][33] = tile[warp];
+  uint32_t v[32];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      uint2 v = __ldg(s2 + q);
-      words[2 * q] = v.x;
-      words[2 * q + 1] = v.y;
+  for (int r = 0; r < 32; ++r) {
+    const int p = 31 - r;
+    const uint8_t* src = base + (int64_t)p * stride;
+    v[r] = 0;
+    if (p >= lo && p < hi) {
+      if (4 * lane + 4 <= nbytes) {
+        v[r] = __ldg(reinterpret_cast<const uint32_t*>(src) + lane);
+      } else if (4 * lane < nbytes) {
+        for (int b = 4 * lane; b < nbytes; ++b) v[r] |= (uint32_t)src[b] << (8 * (b & 3));
+      }
     }
-  } else {
-#pragma unroll
-    for (int q = 0; q < 8; ++q) words[q] = 0;
-    if (take)
-      for (int b = 0; b < nbytes; ++b) words[b >> 2] |= (uint32_t)src[b] << (8 * (b & 3));
   }
-  int32_t* dst = codes + plan.seg_start[level] + first;
 #pragma unroll
-  for (int it = 0; it < 8; ++it) {
-    uint32_t w = warp_transpose32(from_plane_bytes(words[it]), lane);
+  for (int r = 0; r < 32; ++r) tw[r][lane] = v[r];
+  __syncwarp();
+  int32_t* dst = codes + pick4(plan.seg_start, level) + first;
+#pragma unroll 4
+  for (int it = 0; it < 32; ++it) {
+    uint32_t w = warp_transpose32(from_plane_bytes(tw[lane][it]), lane);
     int idx = it * 32 + lane;
     if (idx < count) dst[idx] = sign_inverse(w, nb);
   }
@@ -174,8 +199,10 @@ inverse_bitshuffle_kernel(const uint8_t* __restrict__ planes, int32_t* __restric
 // (`write_pos < res`, :246), which writes zero words past the data and skips
 // some real ones.  Lanes outside the active set read 0 from their partners in
 // the 8-lane network (their register holds the 0 they were initialised with).
-// These kernels run that logic with one CTA of 512 threads and an explicit
-// shared-memory emulation of the shuffle network, so the outcome is fixed.
+// These kernels run that logic with CTAs of 512 threads (one 512-code round
+// each, or all rounds in order in one CTA where rounds overlap) and an
+// explicit shared-memory emulation of the shuffle network, so the outcome is
+// fixed.
 
 __device__ __forceinline__ uint32_t bperm(uint32_t x, uint32_t y, uint32_t s) { return __byte_perm(x, y, s); }
 
@@ -228,7 +255,9 @@ shuffle_last_block_kernel(const int32_t* __restrict__ codes, uint8_t* __restrict
   const int64_t ares = (res + 511) / 512 * 512;
   const int64_t maxa = (last_res_of(g, 0) + 511) / 512 * 512;
   shm[t] = 0;
-  for (int64_t base = 0; base < maxa; base += 512) {
+  // a round only reads words its own round wrote; whether rounds may run in
+  // parallel is decided by the launch (shuffle_last_block_grid)
+  for (int64_t base = (int64_t)blockIdx.x * 512; base < maxa; base += (int64_t)gridDim.x * 512) {
     bool part = base < ares;
     bool ac = part && base + t < res;
     act[t] = ac;
@@ -271,7 +300,7 @@ inverse_last_block_kernel(const uint8_t* __restrict__ planes, int32_t* __restric
   const int64_t start = (g.sh_grid - 1) * (int64_t)kChunk;
   const int64_t res = last_res_of(g, t);
   const int64_t maxr = last_res_of(g, 0);
-  for (int64_t base = 0; base < maxr; base += 512) {
+  for (int64_t base = (int64_t)blockIdx.x * 512; base < maxr; base += (int64_t)gridDim.x * 512) {
     int64_t c = start + base + t;
     bool ac = base + t < res;
     uint32_t v = 0;
@@ -357,6 +386,24 @@ inline int fill_ranges(const Geometry& g, const ShufPlan& plan, ByteRange* out, 
 // overlap (see the oracle): with more blocks than a B200 holds at once
 // (148 SMs x 4 CTAs of 512 threads) it starts after the first wave finished;
 // otherwise the loop round of each side decides.
+// CTAs for the last-block kernels: one per 512-code round
+inline int last_block_rounds(const Geometry& g) {
+  int64_t tail = (int64_t)(g.n % kChunk);
+  if (tail == 0) tail = kChunk;
+  return (int)((tail + g.align_dev + 511) / 512);
+}
+
+// The forward last block's rounds may run concurrently only when no two of
+// them can write the same byte.  Zero words written past the data spill into
+// the first bytes of the next plane; that byte range is also written by the
+// block's own real codes when the block reaches back to within 1024 codes of
+// a level start.  Then the rounds run in order in one CTA, as in the
+// reference, and the later round's byte stands.
+inline int shuffle_last_block_grid(const Geometry& g) {
+  const int64_t start = (g.sh_grid - 1) * (int64_t)kChunk;
+  return start >= g.dprefix[0] + 1024 ? last_block_rounds(g) : 1;
+}
+
 inline bool last_block_lands_last(const Geometry& g) {
   if (g.sh_grid > 148 * 4) return true;
   int64_t tail = (int64_t)(g.n % kChunk);

@@ -13,6 +13,7 @@
 // pass).  All arithmetic uses explicitly rounded intrinsics (fp.cuh) so the
 // results equal the reference build bit for bit.
 #pragma once
+#include <type_traits>
 #include "fp.cuh"
 #include "geometry.h"
 
@@ -57,7 +58,8 @@ struct Expr {
     T s = F::fma(p1, a, F::mul(p2, b));
     s = F::fma(p2, c, s);
     s = F::fma(p1, d, s);
-    return F::div(s, p5);
+    // x/16 and x*0.0625 are the same real number, so they round identically
+    return nat ? F::div(s, p5) : F::mul(s, T(0.0625));
   }
   // (-t0 + 6 t1 + 3 t2) / 8
   static __device__ __forceinline__ T quad_l(T t0, T t1, T t2) {
@@ -85,27 +87,38 @@ struct Expr {
 constexpr int kWin = 17;
 constexpr int kWinVol = kWin * kWin * kWin;
 
-template <class T>
+// FAST marks an interior tile: its whole 17^3 window lies inside the field and
+// it is not the last tile along any axis, so every boundary test below folds
+// to a constant.  Both forms evaluate the same expressions on the same values.
+template <class T, bool FAST = false>
 struct TileCtx {
   T* s;  // shared window, s[(z*17 + y)*17 + x]
   uint32_t gs[3];      // global start of the window (uint32 arithmetic)
-  bool notlast[3];     // the window does not reach the field's end
+  bool notlast_[3];    // the window does not reach the field's end
   uint32_t dim[3];
+  // per-axis fields through selects (a dynamic index would move the context
+  // to local memory)
+  __device__ __forceinline__ bool notlast(int d) const {
+    return FAST ? true : (d == 0 ? notlast_[0] : (d == 1 ? notlast_[1] : notlast_[2]));
+  }
+  __device__ __forceinline__ uint32_t start(int d) const { return d == 0 ? gs[0] : (d == 1 ? gs[1] : gs[2]); }
+  __device__ __forceinline__ uint32_t extent(int d) const { return d == 0 ? dim[0] : (d == 1 ? dim[1] : dim[2]); }
   __device__ __forceinline__ T& at(int x, int y, int z) const { return s[(z * kWin + y) * kWin + x]; }
   __device__ __forceinline__ T get(int axis, int x, int y, int z, int c) const {
     return axis == 0 ? at(c, y, z) : (axis == 1 ? at(x, c, z) : at(x, y, c));
   }
   __device__ __forceinline__ bool in_data(int x, int y, int z) const {
+    if (FAST) return true;
     return gs[0] + (uint32_t)x < dim[0] && gs[1] + (uint32_t)y < dim[1] && gs[2] + (uint32_t)z < dim[2];
   }
   // xyz_predicate (:1173-1185); the exclusive form is used by the last stage
   // of level 0
   __device__ __forceinline__ bool pred_ok(int x, int y, int z, bool inclusive) const {
     if (inclusive) return in_data(x, y, z);
-    return x < 16 && y < 16 && z < 16 + !notlast[2] && in_data(x, y, z);
+    return x < 16 && y < 16 && z < 16 + !notlast(2) && in_data(x, y, z);
   }
   __device__ __forceinline__ bool owned(int x, int y, int z) const {
-    return (x < 16 || !notlast[0]) && (y < 16 || !notlast[1]) && (z < 16 || !notlast[2]);
+    return (x < 16 || !notlast(0)) && (y < 16 || !notlast(1)) && (z < 16 || !notlast(2));
   }
 };
 
@@ -119,13 +132,13 @@ __device__ __forceinline__ int nb_idx(int c, int u, int k) {  // id_x/id_y/id_z 
 }
 
 // 1-D prediction with the per-axis boundary cases (:1300-1326, :1506-1535)
-template <class T>
-__device__ __forceinline__ T pred_line(const TileCtx<T>& t, int axis, int x, int y, int z, int u,
+template <class T, bool FAST>
+__device__ __forceinline__ T pred_line(const TileCtx<T, FAST>& t, int axis, int x, int y, int z, int u,
                                        bool md, bool nat) {
   using E = Expr<T>;
   int ix = axis == 0 ? x : (axis == 1 ? y : z);
-  uint32_t gx = t.gs[axis] + (uint32_t)ix, gs = t.dim[axis];
-  bool c1 = t.notlast[axis];
+  uint32_t gx = t.start(axis) + (uint32_t)ix, gs = t.extent(axis);
+  bool c1 = t.notlast(axis);
   bool c2 = ix >= 3 * u, c3 = ix + 3 * u <= 16;
   bool c4 = gx + 3u * u < gs, c5 = gx + (uint32_t)u < gs;
   T t1 = t.get(axis, x, y, z, nb_idx(ix, u, 1));
@@ -144,18 +157,18 @@ __device__ __forceinline__ T pred_line(const TileCtx<T>& t, int axis, int x, int
 }
 
 // get_interp_order (:1538-1545): 4 cubic, 3 quad-left, 2 quad-right, 1 linear, 0 none
-template <class T>
-__device__ __forceinline__ int interp_order(const TileCtx<T>& t, int axis, int c, int u) {
-  uint32_t gx = t.gs[axis] + (uint32_t)c, gs = t.dim[axis];
-  bool notlast = t.notlast[axis];
+template <class T, bool FAST>
+__device__ __forceinline__ int interp_order(const TileCtx<T, FAST>& t, int axis, int c, int u) {
+  uint32_t gx = t.start(axis) + (uint32_t)c, gs = t.extent(axis);
+  bool notlast = t.notlast(axis);
   int b = c >= 3 * u ? 3 : 1;
   int f = (c + 3 * u <= 16 && (notlast || gx + 3u * u < gs)) ? 3 : ((notlast || gx + (uint32_t)u < gs) ? 1 : 0);
   return b == 3 ? (f == 3 ? 4 : (f == 1 ? 3 : 0)) : (f == 3 ? 2 : (f == 1 ? 1 : 0));
 }
 
 // FACE (:1546-1668)
-template <class T>
-__device__ __forceinline__ T pred_face(const TileCtx<T>& t, int x, int y, int z, int u, bool nat) {
+template <class T, bool FAST>
+__device__ __forceinline__ T pred_face(const TileCtx<T, FAST>& t, int x, int y, int z, int u, bool nat) {
   using E = Expr<T>;
   using F = Fp<T>;
   int a1, a2;
@@ -191,8 +204,8 @@ __device__ __forceinline__ T pred_face(const TileCtx<T>& t, int x, int y, int z,
 }
 
 // CUBE (:1671-1723)
-template <class T>
-__device__ __forceinline__ T pred_cube(const TileCtx<T>& t, int x, int y, int z, int u, bool nat) {
+template <class T, bool FAST>
+__device__ __forceinline__ T pred_cube(const TileCtx<T, FAST>& t, int x, int y, int z, int u, bool nat) {
   using E = Expr<T>;
   using F = Fp<T>;
   int oz = interp_order(t, 2, z, u), oy = interp_order(t, 1, y, u), ox = interp_order(t, 0, x, u);
@@ -230,167 +243,476 @@ __device__ __forceinline__ int32_t quantize(T orig, T pred, T ebr, T ebx2, T* re
   return F::to_int_rz(qt);
 }
 
-template <class T, bool COMPRESS>
-struct StageRunner {
-  const TileCtx<T>& t;
-  const Geometry& g;
-  int32_t* qc;
-  T ebr, ebx2;
-  __device__ __forceinline__ void emit(int x, int y, int z, T pred) const {
-    uint64_t gx = (uint64_t)t.gs[0] + x, gy = (uint64_t)t.gs[1] + y, gz = (uint64_t)t.gs[2] + z;
-    if (COMPRESS) {
-      T rec;
-      int32_t code = quantize(t.at(x, y, z), pred, ebr, ebx2, &rec);
-      t.at(x, y, z) = rec;
-      if (t.owned(x, y, z)) qc[level_major_index(g, gx, gy, gz)] = code;
-    } else {
-      int32_t code = qc[level_major_index(g, gx, gy, gz)];
-      t.at(x, y, z) = Fp<T>::fma(Fp<T>::from_int(code), ebx2, pred);
-    }
-  }
-  // one per-axis sweep (interpolate_stage :1186-1386)
-  __device__ void axis_stage(int axis, int u, int nxs, int xst, int xo, int nys, int yst, int yo,
-                             int nzs, int zst, int zo, bool inclusive, bool nat) const {
-    int total = nxs * nys * nzs;
-    for (int i = threadIdx.x; i < total; i += blockDim.x) {
-      int ii = i % nxs, jj = (i / nxs) % nys, kk = i / nxs / nys;
-      int x = u * (ii * xst + xo), y = u * (jj * yst + yo), z = u * (kk * zst + zo);
-      if (!t.pred_ok(x, y, z, inclusive)) continue;
-      emit(x, y, z, pred_line(t, axis, x, y, z, u, false, nat));
-    }
-    __syncthreads();
-  }
-  // md stages (interpolate_stage_md :1388-1768) with the xyzmap_* point sets
-  __device__ void md_stage(int kind, int u, bool inclusive, bool nat) const {
-    int N = 16 / (2 * u);
-    int total = kind == 1 ? 3 * N * (N + 1) * (N + 1) : (kind == 2 ? 3 * N * N * (N + 1) : N * N * N);
-    for (int i = threadIdx.x; i < total; i += blockDim.x) {
-      int x, y, z;
-      if (kind == 1) {
-        int L = N * (N + 1) * (N + 1), Q = (N + 1) * (N + 1);
-        int grp = i / L, m = i % L, a = m / Q, b = (m % Q) / (N + 1), c = (m % Q) % (N + 1);
-        if (grp == 0) { x = 2 * u * a + u; y = 2 * u * b; z = 2 * u * c; }
-        else if (grp == 1) { x = 2 * u * c; y = 2 * u * a + u; z = 2 * u * b; }
-        else { x = 2 * u * b; y = 2 * u * c; z = 2 * u * a + u; }
-      } else if (kind == 2) {
-        int L = N * N * (N + 1), Q = N * N;
-        int grp = i / L, m = i % L, a = m / Q, b = (m % Q) / N, c = (m % Q) % N;
-        if (grp == 0) { x = 2 * u * a; y = 2 * u * b + u; z = 2 * u * c + u; }
-        else if (grp == 1) { x = 2 * u * c + u; y = 2 * u * a; z = 2 * u * b + u; }
-        else { x = 2 * u * b + u; y = 2 * u * c + u; z = 2 * u * a; }
-      } else {
-        int Q = N * N;
-        x = 2 * u * (i / Q) + u; y = 2 * u * ((i % Q) / N) + u; z = 2 * u * ((i % Q) % N) + u;
-      }
-      if (!t.pred_ok(x, y, z, inclusive)) continue;
-      T pred;
-      if (kind == 1) {
-        int axis = (z % (2 * u)) ? 2 : ((y % (2 * u)) ? 1 : 0);
-        pred = pred_line(t, axis, x, y, z, u, true, nat);
-      } else if (kind == 2) {
-        pred = pred_face(t, x, y, z, u, nat);
-      } else {
-        pred = pred_cube(t, x, y, z, u, nat);
-      }
-      emit(x, y, z, pred);
-    }
-    __syncthreads();
+constexpr int kPredThreads = 256;
+constexpr int kPrefetch = 8;  // independent global loads in flight per thread
+
+// ---- tile sweep --------------------------------------------------------------
+//
+// Every boundary case of pred_line / pred_face / pred_cube depends only on
+// the point's coordinate c along each interpolation axis and on three per-axis
+// limits of the tile:
+//   f3 (the +3u neighbour exists):  c + 3u <= L3  (L3 = 16, or min(16, r-1)
+//                                                  on the field's last tile)
+//   f1 (the +u neighbour exists):   c + u  <= L1  (no limit, or r-1)
+//   in data:                        c < R          (17, or r)
+// where r = extent - tile start.  interp_order (:1538-1545) becomes
+// order = c >= 3u ? (f3 ? 4 : f1 ? 3 : 0) : (f3 ? 2 : f1 ? 1 : 0), and the
+// neighbours sit at fixed offsets from the point in the window.  The functions
+// below evaluate exactly the expressions the generic ones choose, in the same
+// operation order, with the neighbours addressed directly.  For interior tiles
+// (EDGE = false) the limits are constants.  Points are enumerated with an axis
+// the prediction does not interpolate along varying fastest, so a warp mostly
+// shares one formula.
+
+struct AxisLimits {
+  int l3[3], l1[3], r[3];
+};
+
+template <bool EDGE>
+struct Limits {
+  const AxisLimits& a;
+  __device__ __forceinline__ int l3(int d) const { return EDGE ? a.l3[d] : 16; }
+  __device__ __forceinline__ int l1(int d) const { return EDGE ? a.l1[d] : 1 << 20; }
+  __device__ __forceinline__ int r(int d) const { return EDGE ? a.r[d] : kWin; }
+  __device__ __forceinline__ bool in_data(int x, int y, int z) const {
+    return EDGE ? (x < a.r[0] && y < a.r[1] && z < a.r[2]) : true;
   }
 };
 
-// spline_layout_interpolate (:1771-2027)
-template <class T, bool COMPRESS>
-__device__ void run_levels(const TileCtx<T>& t, const Geometry& g, const PredParams<T>& p, int32_t* qc) {
-  int level = 3;
-  for (int u = 8; u >= 1; u >>= 1, --level) {
-    if (level > p.maxlevel) continue;
-    StageRunner<T, COMPRESS> r{t, g, qc, p.ebr[level], p.ebx2[level]};
-    int N = 16 / (2 * u);
-    bool last = level == 0;
-    bool nat = p.natural[level];
-    if (p.use_md[level]) {
-      r.md_stage(1, u, true, nat);
-      r.md_stage(2, u, true, nat);
-      r.md_stage(3, u, !last, nat);
-    } else if (p.reverse[level]) {
-      r.axis_stage(0, u, N, 2, 1, N + 1, 2, 0, N + 1, 2, 0, true, nat);
-      r.axis_stage(1, u, 2 * N + 1, 1, 0, N, 2, 1, N + 1, 2, 0, true, nat);
-      r.axis_stage(2, u, 2 * N + 1, 1, 0, 2 * N + 1, 1, 0, N, 2, 1, !last, nat);
+template <int U, bool EDGE, int D>
+__device__ __forceinline__ int order_of(const Limits<EDGE>& L, int c) {
+  const bool b = c >= 3 * U, f3 = c + 3 * U <= L.l3(D), f1 = c + U <= L.l1(D);
+  return b ? (f3 ? 4 : (f1 ? 3 : 0)) : (f3 ? 2 : (f1 ? 1 : 0));
+}
+
+constexpr int kStride[3] = {1, kWin, kWin * kWin};
+
+// 1-D prediction along window axis D at coordinate c (pred_line :1300-1326)
+template <class T, int U, int D, bool MD>
+__device__ __forceinline__ T line_at(const T* w, int o, bool nat) {
+  using E = Expr<T>;
+  constexpr int S = kStride[D];
+  const T t1 = w[-U * S];
+  if (o == 0) return t1;
+  const T t2 = w[U * S];
+  if (o == 4) {
+    const T t0 = w[-3 * U * S], t3 = w[3 * U * S];
+    return MD ? E::cubic_lambda(t0, t1, t2, t3, nat) : E::cubic_axis(t0, t1, t2, t3, nat);
+  }
+  if (o == 3) return E::quad_l(w[-3 * U * S], t1, t2);
+  if (o == 2) return E::quad_r(t1, t2, w[3 * U * S]);
+  return E::lin(t1, t2);
+}
+
+// FACE (:1546-1668): interpolation along axes D1 (the reference's a1) and D2
+// (a2).  add() is commutative bit for bit, which folds the reference's operand
+// orders into one form.
+template <class T, int U, int D1, int D2>
+__device__ __forceinline__ T face_at(const T* w, int o1, int o2, bool nat) {
+  using E = Expr<T>;
+  using F = Fp<T>;
+  if (o1 == 4 || o2 == 4) {
+    if (o1 != 4) return line_at<T, U, D2, true>(w, o2, nat);
+    if (o2 != 4) return line_at<T, U, D1, true>(w, o1, nat);
+    return E::half(F::add(line_at<T, U, D1, true>(w, o1, nat), line_at<T, U, D2, true>(w, o2, nat)));
+  }
+  if ((o1 >= 2 && o2 >= 2) || (o1 == 1 && o2 == 1))
+    return E::half(F::add(line_at<T, U, D1, true>(w, o1, nat), line_at<T, U, D2, true>(w, o2, nat)));
+  if (o1 >= 2 || (o1 == 1 && o2 == 0)) return line_at<T, U, D1, true>(w, o1, nat);
+  if (o2 >= 1) return line_at<T, U, D2, true>(w, o2, nat);
+  constexpr int S1 = kStride[D1], S2 = kStride[D2];
+  return F::sub(F::add(w[-U * S1], w[-U * S2]), w[-U * S1 - U * S2]);
+}
+
+// CUBE (:1671-1723)
+template <class T, int U>
+__device__ __forceinline__ T cube_at(const T* w, int ox, int oy, int oz, bool nat) {
+  using E = Expr<T>;
+  using F = Fp<T>;
+  auto cub = [&](auto D) {
+    constexpr int s = kStride[decltype(D)::value];
+    return E::cubic_lambda(w[-3 * U * s], w[-U * s], w[U * s], w[3 * U * s], nat);
+  };
+  using DX = std::integral_constant<int, 0>;
+  using DY = std::integral_constant<int, 1>;
+  using DZ = std::integral_constant<int, 2>;
+  if (oz == 4 && oy == 4 && ox == 4) return F::div(F::add(F::add(cub(DX()), cub(DY())), cub(DZ())), T(3));
+  if (oz == 4 && oy == 4) return E::half(F::add(cub(DZ()), cub(DY())));
+  if (oz == 4 && ox == 4) return E::half(F::add(cub(DZ()), cub(DX())));
+  if (oy == 4 && ox == 4) return E::half(F::add(cub(DY()), cub(DX())));
+  if (oz == 4) return cub(DZ());
+  if (oy == 4) return cub(DY());
+  if (ox == 4) return cub(DX());
+  if (ox == 3) return E::quad_l(w[-3 * U], w[-U], w[U]);
+  if (ox == 2) return E::quad_r_cube(w[-U], w[U], w[3 * U]);
+  if (ox == 1) return E::lin(w[-U], w[U]);
+  return w[-U];
+}
+
+// One level (unit U) of a tile sweep.
+template <class T, bool COMPRESS, int U, bool EDGE>
+struct LevelSweep {
+  static constexpr int N = 16 / (2 * U);
+  T* win;
+  int32_t* cw;
+  Limits<EDGE> L;
+  bool zlast;  // the tile is the last along z (exclusive form allows z = 16)
+  T ebr, ebx2;
+  bool nat;
+
+  // The reconstruction keeps each point's code, already converted with
+  // from_int, in the point's own window slot until the point is predicted
+  // (no prediction reads a point of its own or a later stage).
+  __device__ __forceinline__ void emit(int wi, T pred) const {
+    if (COMPRESS) {
+      T rec;
+      cw[wi] = quantize(win[wi], pred, ebr, ebx2, &rec);
+      win[wi] = rec;
     } else {
-      r.axis_stage(2, u, N + 1, 2, 0, N + 1, 2, 0, N, 2, 1, true, nat);
-      r.axis_stage(1, u, N + 1, 2, 0, N, 2, 1, 2 * N + 1, 1, 0, true, nat);
-      r.axis_stage(0, u, N, 2, 1, 2 * N + 1, 1, 0, 2 * N + 1, 1, 0, !last, nat);
+      win[wi] = Fp<T>::fma(win[wi], ebx2, pred);
+    }
+  }
+  // xyz_predicate (:1173-1185)
+  __device__ __forceinline__ bool pred_ok(const int c[3], bool exclusive) const {
+    if (!L.in_data(c[0], c[1], c[2])) return false;
+    return !exclusive || (c[0] < 16 && c[1] < 16 && c[2] < 16 + (EDGE && zlast));
+  }
+  // Per-axis sweep along AX over a box of points.  Dimension d of the box has
+  // ND points at window coordinate U*(k*STD + OFD); dimension 0 varies
+  // fastest and is an axis other than AX.  AXES packs the window axis of
+  // dimensions 0, 1, 2 (two bits each).
+  template <int AX, bool MD, int AXES, int N0, int ST0, int OF0, int N1, int ST1, int OF1, int N2, int ST2, int OF2,
+            bool SYNC = true>
+  __device__ __forceinline__ void sweep(bool exclusive) const {
+    constexpr int total = N0 * N1 * N2;
+    constexpr int A0 = AXES & 3, A1 = (AXES >> 2) & 3, A2 = (AXES >> 4) & 3;
+#pragma unroll 2
+    for (int i = threadIdx.x; i < total; i += kPredThreads) {
+      const int k0 = i % N0, k1 = (i / N0) % N1, k2 = i / (N0 * N1);
+      int c[3];
+      c[A0] = U * (k0 * ST0 + OF0);
+      c[A1] = U * (k1 * ST1 + OF1);
+      c[A2] = U * (k2 * ST2 + OF2);
+      if (!pred_ok(c, exclusive)) continue;
+      const int wi = (c[2] * kWin + c[1]) * kWin + c[0];
+      emit(wi, line_at<T, U, AX, MD>(win + wi, order_of<U, EDGE, AX>(L, c[AX]), nat));
+    }
+    if (SYNC) __syncthreads();
+  }
+  // md faces: the point is even along axis E (dimension 0, fastest) and odd
+  // along the two interpolation axes P1 (the reference's a1) and P2 (a2)
+  template <int E, int P1, int P2, bool SYNC = true>
+  __device__ __forceinline__ void faces() const {
+    constexpr int total = (N + 1) * N * N;
+#pragma unroll 2
+    for (int i = threadIdx.x; i < total; i += kPredThreads) {
+      const int k0 = i % (N + 1), k1 = (i / (N + 1)) % N, k2 = i / ((N + 1) * N);
+      int c[3];
+      c[E] = 2 * U * k0;
+      c[P1] = 2 * U * k1 + U;
+      c[P2] = 2 * U * k2 + U;
+      if (!pred_ok(c, false)) continue;
+      const int wi = (c[2] * kWin + c[1]) * kWin + c[0];
+      emit(wi, face_at<T, U, P1, P2>(win + wi, order_of<U, EDGE, P1>(L, c[P1]), order_of<U, EDGE, P2>(L, c[P2]),
+                                      nat));
+    }
+    if (SYNC) __syncthreads();
+  }
+  __device__ __forceinline__ void cube(bool exclusive) const {
+    constexpr int total = N * N * N;
+#pragma unroll 2
+    for (int i = threadIdx.x; i < total; i += kPredThreads) {
+      int c[3] = {2 * U * (i % N) + U, 2 * U * ((i / N) % N) + U, 2 * U * (i / (N * N)) + U};
+      if (!pred_ok(c, exclusive)) continue;
+      const int wi = (c[2] * kWin + c[1]) * kWin + c[0];
+      emit(wi, cube_at<T, U>(win + wi, order_of<U, EDGE, 0>(L, c[0]), order_of<U, EDGE, 1>(L, c[1]),
+                             order_of<U, EDGE, 2>(L, c[2]), nat));
+    }
+    __syncthreads();
+  }
+  // the three stages of the level (spline_layout_interpolate :1771-2027)
+  __device__ __forceinline__ void run(bool md, bool rev) const {
+    constexpr bool kLast = U == 1;
+    // axis codes: x = 0, y = 1, z = 2; AXES = a0 | a1 << 2 | a2 << 4
+    if (md) {
+      // lines (xyzmap_line): x-lines vary y fastest, y- and z-lines vary x.
+      // Points of one stage only read coarser points, so the three groups
+      // share one barrier.
+      sweep<0, true, 1 | (2 << 2) | (0 << 4), N + 1, 2, 0, N + 1, 2, 0, N, 2, 1, false>(false);
+      sweep<1, true, 0 | (2 << 2) | (1 << 4), N + 1, 2, 0, N + 1, 2, 0, N, 2, 1, false>(false);
+      sweep<2, true, 0 | (1 << 2) | (2 << 4), N + 1, 2, 0, N + 1, 2, 0, N, 2, 1>(false);
+      // faces (xyzmap_face): x even -> z,y; y even -> z,x; z even -> y,x
+      faces<0, 2, 1, false>();
+      faces<1, 2, 0, false>();
+      faces<2, 1, 0>();
+      cube(kLast);
+    } else if (rev) {
+      // x: (x odd, y even, z even), vary y fastest
+      sweep<0, false, 1 | (0 << 2) | (2 << 4), N + 1, 2, 0, N, 2, 1, N + 1, 2, 0>(false);
+      // y: (x any, y odd, z even), vary x
+      sweep<1, false, 0 | (1 << 2) | (2 << 4), 2 * N + 1, 1, 0, N, 2, 1, N + 1, 2, 0>(false);
+      // z: (x any, y any, z odd), vary x
+      sweep<2, false, 0 | (1 << 2) | (2 << 4), 2 * N + 1, 1, 0, 2 * N + 1, 1, 0, N, 2, 1>(kLast);
+    } else {
+      // z: (x even, y even, z odd), vary x
+      sweep<2, false, 0 | (1 << 2) | (2 << 4), N + 1, 2, 0, N + 1, 2, 0, N, 2, 1>(false);
+      // y: (x even, y odd, z any), vary x
+      sweep<1, false, 0 | (1 << 2) | (2 << 4), N + 1, 2, 0, N, 2, 1, 2 * N + 1, 1, 0>(false);
+      // x: (x odd, y any, z any), vary y
+      sweep<0, false, 1 | (0 << 2) | (2 << 4), 2 * N + 1, 1, 0, N, 2, 1, 2 * N + 1, 1, 0>(kLast);
+    }
+  }
+};
+
+template <class T, bool COMPRESS, bool EDGE, int U, int LEVEL>
+__device__ __forceinline__ void sweep_level(T* win, int32_t* cw, const AxisLimits& lim, bool zlast,
+                                            const PredParams<T>& p) {
+  if (LEVEL > p.maxlevel) return;
+  LevelSweep<T, COMPRESS, U, EDGE> lv{win, cw, Limits<EDGE>{lim}, zlast, p.ebr[LEVEL], p.ebx2[LEVEL],
+                                      p.natural[LEVEL] != 0};
+  lv.run(p.use_md[LEVEL] != 0, p.reverse[LEVEL] != 0);
+}
+
+// spline_layout_interpolate (:1771-2027): levels 3..0
+template <class T, bool COMPRESS, bool EDGE>
+__device__ void sweep_levels(T* win, int32_t* cw, const AxisLimits& lim, bool zlast, const PredParams<T>& p) {
+  sweep_level<T, COMPRESS, EDGE, 8, 3>(win, cw, lim, zlast, p);
+  sweep_level<T, COMPRESS, EDGE, 4, 2>(win, cw, lim, zlast, p);
+  sweep_level<T, COMPRESS, EDGE, 2, 1>(win, cw, lim, zlast, p);
+  sweep_level<T, COMPRESS, EDGE, 1, 0>(win, cw, lim, zlast, p);
+}
+
+// ---- tiles -------------------------------------------------------------------
+
+// Tiles are launched in two parts so that each kernel runs one code path:
+// part 0 = interior tiles ((ax-1)(ay-1)(az-1) of them), part 1 = the tiles
+// on the last slab along z, then y, then x.
+PRISM_HD uint64_t tiles_in_part(const Geometry& g, int part) {
+  uint64_t inner = (uint64_t)(g.ax - 1) * (g.ay - 1) * (g.az - 1);
+  return part == 0 ? inner : (uint64_t)g.ax * g.ay * g.az - inner;
+}
+
+template <int PART>
+__device__ __forceinline__ void tile_of_block(const Geometry& g, uint32_t bi[3]) {
+  uint32_t j = blockIdx.x;
+  if (PART == 0) {
+    bi[0] = j % (g.ax - 1); bi[1] = (j / (g.ax - 1)) % (g.ay - 1); bi[2] = j / ((g.ax - 1) * (g.ay - 1));
+    return;
+  }
+  if (j < g.ax * g.ay) { bi[0] = j % g.ax; bi[1] = j / g.ax; bi[2] = g.az - 1; return; }
+  j -= g.ax * g.ay;
+  if (j < g.ax * (g.az - 1)) { bi[0] = j % g.ax; bi[1] = g.ay - 1; bi[2] = j / g.ax; return; }
+  j -= g.ax * (g.az - 1);
+  bi[0] = g.ax - 1; bi[1] = j % (g.ay - 1); bi[2] = j / (g.ay - 1);
+}
+
+// Per-tile frame: window origin, limits, and the level-0 slot of each window
+// row (y, z) at x = 0 (level-major order, :2070-2085), which makes the slot of
+// a level-0 point one add.
+struct TileFrame {
+  uint32_t gs[3];
+  bool last[3];
+  AxisLimits lim;
+};
+
+__device__ __forceinline__ void tile_frame(const Geometry& g, const uint32_t bi[3], TileFrame& f) {
+  const uint32_t gd[3] = {g.ax, g.ay, g.az}, dim[3] = {g.nx, g.ny, g.nz};
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    f.gs[d] = bi[d] * 16u;
+    f.last[d] = bi[d] == gd[d] - 1;
+    int r = (int)min(dim[d] - f.gs[d], 17u);
+    f.lim.r[d] = f.last[d] ? r : kWin;
+    f.lim.l3[d] = f.last[d] ? min(16, r - 1) : 16;
+    f.lim.l1[d] = f.last[d] ? r - 1 : 1 << 20;
+  }
+}
+
+__device__ __forceinline__ void win_xyz(int i, int& x, int& y, int& z) {
+  x = i % kWin; y = (i / kWin) % kWin; z = i / (kWin * kWin);
+}
+
+// level of a window point: 0..3, or 4 for the stride-16 anchors (the window
+// starts on a multiple of 16, so window and global coordinates agree mod 16)
+__device__ __forceinline__ int win_level(int x, int y, int z) { return __ffs(x | y | z | 16) - 1; }
+
+// Level-major slot of a point whose level (0..3) is known (the formula of
+// level_major_index without its level search).
+__device__ __forceinline__ uint64_t lm_slot(const Geometry& g, int level, uint64_t gx, uint64_t gy, uint64_t gz) {
+  gx >>= level; gy >>= level; gz >>= level;
+  uint64_t gid = gx + gy * g.leaps[level][0] + gz * g.leaps[level][1];
+  gid += g.lm_prefix[level] - ((gz + 1) >> 1) * g.leaps[level + 1][1] -
+         (uint64_t)((gz & 1) == 0) * ((gy + 1) >> 1) * g.leaps[level + 1][0] -
+         (uint64_t)(((gz | gy) & 1) == 0) * ((gx + 1) >> 1);
+  return gid;
+}
+
+// Row table: rows[(z*17 + y)] = level-0 slot of window point (0, y, z) minus
+// the x-dependent part, so that a level-0 point's slot is
+// rows[row] + x - (y, z both even ? (x + 1) / 2 : 0) (x, gs[0] even).
+__device__ __forceinline__ void fill_rows(const Geometry& g, const TileFrame& f, uint64_t* rows) {
+  for (int r = threadIdx.x; r < kWin * kWin; r += kPredThreads) {
+    const uint64_t gy = f.gs[1] + r % kWin, gz = f.gs[2] + r / kWin;
+    uint64_t base = (uint64_t)f.gs[0] + gy * g.leaps[0][0] + gz * g.leaps[0][1] + g.lm_prefix[0] -
+                    ((gz + 1) >> 1) * g.leaps[1][1] - (uint64_t)((gz & 1) == 0) * ((gy + 1) >> 1) * g.leaps[1][0];
+    if (((gz | gy) & 1) == 0) base -= f.gs[0] >> 1;
+    rows[r] = base;
+  }
+}
+
+__device__ __forceinline__ uint64_t slot_of(const Geometry& g, const TileFrame& f, const uint64_t* rows, int lv,
+                                            int x, int y, int z) {
+  if (lv == 0) {
+    const int row = z * kWin + y;
+    return rows[row] + (uint64_t)x - ((((y | z) & 1) == 0) ? (uint64_t)((x + 1) >> 1) : 0);
+  }
+  return lm_slot(g, lv, (uint64_t)f.gs[0] + x, (uint64_t)f.gs[1] + y, (uint64_t)f.gs[2] + z);
+}
+
+// Shared memory of a compression tile: the value window, the codes in the
+// same shape and the row table (~61 KB for double, ~42 KB for float).
+template <class T>
+struct CompressSmem {
+  T win[kWinVol];
+  int32_t cw[kWinVol];
+  uint64_t rows[kWin * kWin];
+  PredParams<T> p;
+};
+
+// Shared memory of a reconstruction tile: the window (codes travel in the
+// window slots) and the row table (~42 KB for double, ~22 KB for float).
+template <class T>
+struct ReconSmem {
+  T win[kWinVol];
+  uint64_t rows[kWin * kWin];
+  PredParams<T> p;
+};
+
+// Compression: data -> anchors + level-major codes (interpolation :2137-2173).
+// The window is loaded with kPrefetch independent loads per thread in flight,
+// the 12 stages run in shared memory, and the codes of the points the tile
+// owns leave in one pass at the end.
+template <class T, int PART>
+__global__ void __launch_bounds__(kPredThreads)
+predict_compress_kernel(const T* __restrict__ data, Geometry g, const PredParams<T>* __restrict__ pp,
+                        T* __restrict__ anchors, int32_t* __restrict__ qc) {
+  constexpr bool EDGE = PART == 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  CompressSmem<T>& sm = *reinterpret_cast<CompressSmem<T>*>(smem_raw);
+  uint32_t bi[3];
+  tile_of_block<PART>(g, bi);
+  TileFrame f;
+  tile_frame(g, bi, f);
+  const Limits<EDGE> L{f.lim};
+  const int tid = threadIdx.x;
+  if (tid == 0) sm.p = *pp;
+  fill_rows(g, f, sm.rows);
+  const uint64_t sy = g.nx, sz = (uint64_t)g.nx * g.ny;
+  const T* base = data + (uint64_t)f.gs[0] + (uint64_t)f.gs[1] * sy + (uint64_t)f.gs[2] * sz;
+  for (int b = tid; b < kWinVol; b += kPrefetch * kPredThreads) {
+    T v[kPrefetch];
+#pragma unroll
+    for (int k = 0; k < kPrefetch; ++k) {
+      int i = b + k * kPredThreads, x, y, z;
+      win_xyz(i, x, y, z);
+      v[k] = T(0);
+      if (i < kWinVol && L.in_data(x, y, z)) v[k] = __ldg(base + x + (uint64_t)y * sy + (uint64_t)z * sz);
+    }
+#pragma unroll
+    for (int k = 0; k < kPrefetch; ++k)
+      if (b + k * kPredThreads < kWinVol) sm.win[b + k * kPredThreads] = v[k];
+  }
+  __syncthreads();
+  if (tid == 0) anchors[bi[0] + (uint64_t)bi[1] * g.ax + (uint64_t)bi[2] * g.ax * g.ay] = sm.win[0];
+  sweep_levels<T, true, EDGE>(sm.win, sm.cw, f.lim, f.last[2], sm.p);
+  // every non-anchor point of the tile's own region that lies in the field
+  // was emitted; the region is 16^3, plus the plane at 16 on a last tile
+  const int xs = 16 + (EDGE && f.last[0]), ys = 16 + (EDGE && f.last[1]), zs = 16 + (EDGE && f.last[2]);
+  const int total = xs * ys * zs;
+  for (int i = tid; i < total; i += kPredThreads) {
+    const int x = i % xs, y = (i / xs) % ys, z = i / (xs * ys);
+    const int lv = win_level(x, y, z);
+    if (lv == 4 || !L.in_data(x, y, z)) continue;
+    qc[slot_of(g, f, sm.rows, lv, x, y, z)] = sm.cw[(z * kWin + y) * kWin + x];
+  }
+}
+
+// Reconstruction: anchors + codes -> values (interpolation_reverse
+// :2177-2207); PROG adds the previous values (interpolation_progressive_reverse
+// :2209-2239, shmem2global_data_progressive :1123-1147).  All codes the tile
+// can use are fetched up front with kPrefetch loads in flight per thread.
+template <class T, bool PROG, int PART>
+__global__ void __launch_bounds__(kPredThreads, 5)
+reconstruct_kernel(const int32_t* __restrict__ qc, const T* __restrict__ anchors, Geometry g,
+                   const PredParams<T>* __restrict__ pp, const T* old, T* out) {
+  constexpr bool EDGE = PART == 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  ReconSmem<T>& sm = *reinterpret_cast<ReconSmem<T>*>(smem_raw);
+  uint32_t bi[3];
+  tile_of_block<PART>(g, bi);
+  TileFrame f;
+  tile_frame(g, bi, f);
+  const Limits<EDGE> L{f.lim};
+  const int tid = threadIdx.x;
+  const int maxlevel = pp->maxlevel;
+  if (tid == 0) sm.p = *pp;
+  fill_rows(g, f, sm.rows);
+  __syncthreads();
+  for (int b = tid; b < kWinVol; b += kPrefetch * kPredThreads) {
+    int32_t v[kPrefetch];
+#pragma unroll
+    for (int k = 0; k < kPrefetch; ++k) {
+      int i = b + k * kPredThreads, x, y, z;
+      win_xyz(i, x, y, z);
+      v[k] = 0;
+      const int lv = win_level(x, y, z);
+      if (i < kWinVol && lv < 4 && lv <= maxlevel && L.in_data(x, y, z))
+        v[k] = __ldg(qc + slot_of(g, f, sm.rows, lv, x, y, z));
+    }
+#pragma unroll
+    for (int k = 0; k < kPrefetch; ++k) {
+      int i = b + k * kPredThreads;
+      if (i < kWinVol) sm.win[i] = Fp<T>::from_int(v[k]);
+    }
+  }
+  __syncthreads();
+  if (tid < 8) {  // x_reset_scratch_data (:1027-1067): anchors at the corners
+    int x = (tid & 1) * 16, y = ((tid >> 1) & 1) * 16, z = (tid >> 2) * 16;
+    uint32_t ax = x / 16 + bi[0], ay = y / 16 + bi[1], az = z / 16 + bi[2];
+    if (ax < g.ax && ay < g.ay && az < g.az)
+      sm.win[(z * kWin + y) * kWin + x] = anchors[ax + (uint64_t)ay * g.ax + (uint64_t)az * g.ax * g.ay];
+  }
+  __syncthreads();
+  sweep_levels<T, false, EDGE>(sm.win, nullptr, f.lim, f.last[2], sm.p);
+  const uint64_t sy = g.nx, sz = (uint64_t)g.nx * g.ny;
+  const uint64_t base = (uint64_t)f.gs[0] + (uint64_t)f.gs[1] * sy + (uint64_t)f.gs[2] * sz;
+  const int xs = 16 + (EDGE && f.last[0]), ys = 16 + (EDGE && f.last[1]), zs = 16 + (EDGE && f.last[2]);
+  const int total = xs * ys * zs;
+  for (int b = tid; b < total; b += kPrefetch * kPredThreads) {
+    T o[kPrefetch];
+    if (PROG) {
+#pragma unroll
+      for (int k = 0; k < kPrefetch; ++k) {
+        int i = b + k * kPredThreads;
+        int x = i % xs, y = (i / xs) % ys, z = i / (xs * ys);
+        o[k] = T(0);
+        if (i < total && L.in_data(x, y, z)) o[k] = old[base + x + (uint64_t)y * sy + (uint64_t)z * sz];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kPrefetch; ++k) {
+      int i = b + k * kPredThreads;
+      int x = i % xs, y = (i / xs) % ys, z = i / (xs * ys);
+      if (i >= total || !L.in_data(x, y, z)) continue;
+      T v = sm.win[(z * kWin + y) * kWin + x];
+      out[base + x + (uint64_t)y * sy + (uint64_t)z * sz] = PROG ? Fp<T>::add(v, o[k]) : v;
     }
   }
 }
 
-constexpr int kPredThreads = 256;
-
-// Compression: data -> anchors + level-major codes.
 template <class T>
-__global__ void __launch_bounds__(kPredThreads)
-predict_compress_kernel(const T* __restrict__ data, Geometry g, const PredParams<T>* __restrict__ pp,
-                        T* __restrict__ anchors, int32_t* __restrict__ qc) {
-  __shared__ T win[kWinVol];
-  __shared__ PredParams<T> p;
-  uint32_t tile = blockIdx.x;
-  TileCtx<T> t;
-  t.s = win;
-  uint32_t bi[3] = {tile % g.ax, (tile / g.ax) % g.ay, tile / g.ax / g.ay};
-  uint32_t gd[3] = {g.ax, g.ay, g.az};
-  t.dim[0] = g.nx; t.dim[1] = g.ny; t.dim[2] = g.nz;
-#pragma unroll
-  for (int d = 0; d < 3; ++d) { t.gs[d] = bi[d] * 16u; t.notlast[d] = bi[d] != gd[d] - 1; }
-  if (threadIdx.x == 0) p = *pp;
-  const uint64_t sy = g.nx, sz = (uint64_t)g.nx * g.ny;
-  for (int i = threadIdx.x; i < kWinVol; i += blockDim.x) {
-    int x = i % kWin, y = (i / kWin) % kWin, z = i / (kWin * kWin);
-    T v = T(0);
-    if (t.in_data(x, y, z))
-      v = data[((uint64_t)t.gs[0] + x) + ((uint64_t)t.gs[1] + y) * sy + ((uint64_t)t.gs[2] + z) * sz];
-    win[i] = v;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) anchors[bi[0] + (uint64_t)bi[1] * g.ax + (uint64_t)bi[2] * g.ax * g.ay] = win[0];
-  run_levels<T, true>(t, g, p, qc);
-}
-
-// Reconstruction: anchors + codes -> values; PROG adds the previous values
-// (shmem2global_data_progressive :1123-1147).
-template <class T, bool PROG>
-__global__ void __launch_bounds__(kPredThreads)
-reconstruct_kernel(const int32_t* __restrict__ qc, const T* __restrict__ anchors, Geometry g,
-                   const PredParams<T>* __restrict__ pp, const T* old, T* out) {
-  __shared__ T win[kWinVol];
-  __shared__ PredParams<T> p;
-  uint32_t tile = blockIdx.x;
-  TileCtx<T> t;
-  t.s = win;
-  uint32_t bi[3] = {tile % g.ax, (tile / g.ax) % g.ay, tile / g.ax / g.ay};
-  uint32_t gd[3] = {g.ax, g.ay, g.az};
-  t.dim[0] = g.nx; t.dim[1] = g.ny; t.dim[2] = g.nz;
-#pragma unroll
-  for (int d = 0; d < 3; ++d) { t.gs[d] = bi[d] * 16u; t.notlast[d] = bi[d] != gd[d] - 1; }
-  if (threadIdx.x == 0) p = *pp;
-  for (int i = threadIdx.x; i < kWinVol; i += blockDim.x) win[i] = T(0);
-  __syncthreads();
-  if (threadIdx.x < 8) {  // x_reset_scratch_data (:1027-1067): anchors at the corners
-    int x = (threadIdx.x & 1) * 16, y = ((threadIdx.x >> 1) & 1) * 16, z = (threadIdx.x >> 2) * 16;
-    uint32_t ax = x / 16 + bi[0], ay = y / 16 + bi[1], az = z / 16 + bi[2];
-    if (ax < g.ax && ay < g.ay && az < g.az) win[(z * kWin + y) * kWin + x] = anchors[ax + (uint64_t)ay * g.ax + (uint64_t)az * g.ax * g.ay];
-  }
-  __syncthreads();
-  run_levels<T, false>(t, g, p, const_cast<int32_t*>(qc));
-  const uint64_t sy = g.nx, sz = (uint64_t)g.nx * g.ny;
-  int xs = 16 + !t.notlast[0], ys = 16 + !t.notlast[1], zs = 16 + !t.notlast[2];
-  int total = xs * ys * zs;
-  for (int i = threadIdx.x; i < total; i += blockDim.x) {
-    int x = i % xs, y = (i / xs) % ys, z = i / (xs * ys);
-    if (!t.in_data(x, y, z)) continue;
-    uint64_t gid = ((uint64_t)t.gs[0] + x) + ((uint64_t)t.gs[1] + y) * sy + ((uint64_t)t.gs[2] + z) * sz;
-    T v = t.at(x, y, z);
-    out[gid] = PROG ? Fp<T>::add(v, old[gid]) : v;
-  }
-}
+constexpr int compress_smem_bytes() { return (int)sizeof(CompressSmem<T>); }
+template <class T>
+constexpr int recon_smem_bytes() { return (int)sizeof(ReconSmem<T>); }
 
 }  // namespace prism_b200

@@ -161,6 +161,56 @@ static uint64_t qc_len(const Geometry& g) {
 
 static Small* small(prism_handle* h) { return h->small.as<Small>(); }
 
+// Raise a kernel's dynamic shared-memory limit, once per device.
+template <auto Kernel>
+static cudaError_t smem_limit(int bytes) {
+  static std::mutex m;
+  static bool done[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaFuncSetAttribute(Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  std::lock_guard<std::mutex> lock(m);
+  if (!done[dev]) {
+    e = cudaFuncSetAttribute(Kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
+    done[dev] = true;
+  }
+  return cudaSuccess;
+}
+
+// The tile kernels run as two launches: interior tiles (part 0) and the tiles
+// on the field's last slabs (part 1).
+template <class T>
+static int launch_predict(prism_handle* h, const T* in, const Geometry& g, const PredParams<T>* pp, T* anchors,
+                          int32_t* qc, cudaStream_t st) {
+  const int smem = compress_smem_bytes<T>();
+  constexpr auto k0 = predict_compress_kernel<T, 0>;
+  constexpr auto k1 = predict_compress_kernel<T, 1>;
+  CK(smem_limit<k0>(smem));
+  CK(smem_limit<k1>(smem));
+  uint64_t n0 = tiles_in_part(g, 0), n1 = tiles_in_part(g, 1);
+  if (n0) { k0<<<(unsigned)n0, kPredThreads, smem, st>>>(in, g, pp, anchors, qc); h->launches += 1; }
+  if (n1) { k1<<<(unsigned)n1, kPredThreads, smem, st>>>(in, g, pp, anchors, qc); h->launches += 1; }
+  CK(cudaGetLastError());
+  return PRISM_OK;
+}
+
+template <class T, bool PROG>
+static int launch_reconstruct(prism_handle* h, const int32_t* qc, const T* anchors, const Geometry& g,
+                              const PredParams<T>* pp, const T* old, T* out, cudaStream_t st) {
+  const int smem0 = recon_smem_bytes<T>(), smem1 = recon_smem_bytes<T>();
+  constexpr auto k0 = reconstruct_kernel<T, PROG, 0>;
+  constexpr auto k1 = reconstruct_kernel<T, PROG, 1>;
+  CK(smem_limit<k0>(smem0));
+  CK(smem_limit<k1>(smem1));
+  uint64_t n0 = tiles_in_part(g, 0), n1 = tiles_in_part(g, 1);
+  if (n0) { k0<<<(unsigned)n0, kPredThreads, smem0, st>>>(qc, anchors, g, pp, old, out); h->launches += 1; }
+  if (n1) { k1<<<(unsigned)n1, kPredThreads, smem1, st>>>(qc, anchors, g, pp, old, out); h->launches += 1; }
+  CK(cudaGetLastError());
+  return PRISM_OK;
+}
+
 static int ensure_common(prism_handle* h, const Geometry& g) {
   CKA(h->qc.ensure(qc_len(g) * sizeof(int32_t)));
   CKA(h->planes.ensure(g.aligned_size + 64));
@@ -274,12 +324,12 @@ static int launch_bitshuffle(prism_handle* h, const int32_t* qc, const Geometry&
   }
   const int32_t* codes = qc + g.anchors;
   bool last_last = last_block_lands_last(g);
-  if (!last_last) shuffle_last_block_kernel<<<1, 512, 0, st>>>(codes, planes, g, nb, g.aligned_size);
+  if (!last_last) shuffle_last_block_kernel<<<shuffle_last_block_grid(g), 512, 0, st>>>(codes, planes, g, nb, g.aligned_size);
   if (plan.items > 0) {
     int64_t blocks = (plan.items + kShufWarps - 1) / kShufWarps;
     bitshuffle_kernel<<<(unsigned)blocks, kShufWarps * 32, 0, st>>>(codes, planes, g, plan, nb);
   }
-  if (last_last) shuffle_last_block_kernel<<<1, 512, 0, st>>>(codes, planes, g, nb, g.aligned_size);
+  if (last_last) shuffle_last_block_kernel<<<shuffle_last_block_grid(g), 512, 0, st>>>(codes, planes, g, nb, g.aligned_size);
   prof_end(h, kStShuffle, st);
   h->launches += 1 + (plan.items > 0);
   CK(cudaGetLastError());
@@ -301,7 +351,7 @@ static int launch_inverse(prism_handle* h, const uint8_t* planes, const Geometry
     inverse_bitshuffle_kernel<<<(unsigned)blocks, kShufWarps * 32, 0, st>>>(planes, codes, g, plan, nb, dbegin, dend);
     h->launches += 1;
   }
-  inverse_last_block_kernel<<<1, 512, 0, st>>>(planes, codes, g, nb, dbegin, dend, g.aligned_size);
+  inverse_last_block_kernel<<<last_block_rounds(g), 512, 0, st>>>(planes, codes, g, nb, dbegin, dend, g.aligned_size);
   prof_end(h, kStInverse, st);
   h->launches += 1;
   CK(cudaGetLastError());
@@ -407,11 +457,9 @@ static int compress_t(prism_handle* h, const T* in, const Geometry& g, int mode,
   rc = zero_code_padding(h, g, st);
   if (rc) return rc;
   prof_begin(h, kStPredict, st);
-  predict_compress_kernel<T><<<(unsigned)g.anchors, kPredThreads, 0, st>>>(in, g, params_ptr<T>(h), h->anchors.as<T>(),
-                                                                            h->qc.as<int32_t>());
+  rc = launch_predict<T>(h, in, g, params_ptr<T>(h), h->anchors.as<T>(), h->qc.as<int32_t>(), st);
+  if (rc) return rc;
   prof_end(h, kStPredict, st);
-  h->launches += 1;
-  CK(cudaGetLastError());
   rc = launch_bitshuffle(h, h->qc.as<int32_t>(), g, nb, h->planes.as<uint8_t>(), st);
   if (rc) return rc;
   rc = launch_encode(h, h->planes.as<uint8_t>(), g, out, st);
@@ -448,10 +496,11 @@ static int decompress_t(prism_handle* h, const uint8_t* cont, uint64_t size, con
   rc = launch_inverse(h, h->planes.as<uint8_t>(), g, 0 /*SM*/, nullptr, nullptr, h->qc.as<int32_t>(), st);
   if (rc) return rc;
   prof_begin(h, kStReconstruct, st);
-  reconstruct_kernel<T, false><<<(unsigned)g.anchors, kPredThreads, 0, st>>>(
-      h->qc.as<int32_t>(), reinterpret_cast<const T*>(tr + 1040), g, params_ptr<T>(h), nullptr, out);
+  rc = launch_reconstruct<T, false>(h, h->qc.as<int32_t>(), reinterpret_cast<const T*>(tr + 1040), g,
+                                    params_ptr<T>(h), nullptr, out, st);
+  if (rc) return rc;
   prof_end(h, kStReconstruct, st);
-  h->launches += 2;
+  h->launches += 1;
   CK(cudaGetLastError());
   return finish(h, st);
 }
@@ -660,16 +709,15 @@ static int progressive_step_t(prism_prog* p, double target, T* values, cudaStrea
   if (rc) return rc;
   prof_begin(h, kStReconstruct, st);
   if (first) {
-    reconstruct_kernel<T, false><<<(unsigned)g.anchors, kPredThreads, 0, st>>>(
-        h->qc.as<int32_t>(), reinterpret_cast<const T*>(tr + 1040), g, params_ptr<T>(h), nullptr, values);
+    rc = launch_reconstruct<T, false>(h, h->qc.as<int32_t>(), reinterpret_cast<const T*>(tr + 1040), g,
+                                      params_ptr<T>(h), nullptr, values, st);
   } else {
     CK(cudaMemsetAsync(h->zero_anchors.p, 0, g.anchors * sizeof(T), st));
-    reconstruct_kernel<T, true><<<(unsigned)g.anchors, kPredThreads, 0, st>>>(
-        h->qc.as<int32_t>(), h->zero_anchors.as<T>(), g, params_ptr<T>(h), values, values);
+    rc = launch_reconstruct<T, true>(h, h->qc.as<int32_t>(), h->zero_anchors.as<T>(), g, params_ptr<T>(h), values,
+                                     values, st);
   }
+  if (rc) return rc;
   prof_end(h, kStReconstruct, st);
-  h->launches += 1;
-  CK(cudaGetLastError());
   CK(cudaMemcpyAsync(&p->state, &s->sstate, sizeof(StrategyState), cudaMemcpyDeviceToHost, st));
   rc = finish(h, st);
   if (rc) return rc;
@@ -750,8 +798,8 @@ static int predict_stage_t(prism_handle* h, const T* in, const Geometry& g, doub
   set_double_kernel<<<1, 1, 0, st>>>(&s->range, 1.0);
   params_kernel<T><<<1, 32, 0, st>>>(0, eb, &s->range, alpha_of(rel_eb), nullptr, 0, s->params + 200, 4,
                                      reinterpret_cast<PredParams<T>*>(s->params), nullptr, &s->eb);
-  predict_compress_kernel<T><<<(unsigned)g.anchors, kPredThreads, 0, st>>>(in, g, params_ptr<T>(h), anchors, codes);
-  CK(cudaGetLastError());
+  rc = launch_predict<T>(h, in, g, params_ptr<T>(h), anchors, codes, st);
+  if (rc) return rc;
   return finish(h, st);
 }
 
@@ -777,11 +825,9 @@ static int reconstruct_stage_t(prism_handle* h, const int32_t* codes, const T* a
   set_double_kernel<<<1, 1, 0, st>>>(&s->range, 1.0);
   params_kernel<T><<<1, 32, 0, st>>>(0, eb, &s->range, alpha_of(rel_eb), nullptr, 0, s->params + 200, maxlevel,
                                      reinterpret_cast<PredParams<T>*>(s->params), nullptr, &s->eb);
-  if (old)
-    reconstruct_kernel<T, true><<<(unsigned)g.anchors, kPredThreads, 0, st>>>(codes, anchors, g, params_ptr<T>(h), old, out);
-  else
-    reconstruct_kernel<T, false><<<(unsigned)g.anchors, kPredThreads, 0, st>>>(codes, anchors, g, params_ptr<T>(h), nullptr, out);
-  CK(cudaGetLastError());
+  rc = old ? launch_reconstruct<T, true>(h, codes, anchors, g, params_ptr<T>(h), old, out, st)
+           : launch_reconstruct<T, false>(h, codes, anchors, g, params_ptr<T>(h), nullptr, out, st);
+  if (rc) return rc;
   return finish(h, st);
 }
 
