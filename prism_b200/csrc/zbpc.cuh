@@ -65,30 +65,26 @@ __device__ __forceinline__ int warp_incl_scan(int v, int lane) {
   return v;
 }
 
-// exclusive prefix over the block; *total receives the block sum
+// exclusive prefix over the block; *total receives the block sum.  Two
+// barriers; scratch must not be reused before the next barrier.
 __device__ __forceinline__ int block_excl_scan(int v, int* scratch, int* total) {
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int incl = warp_incl_scan(v, lane);
   if (lane == 31) scratch[warp] = incl;
   __syncthreads();
-  if (warp == 0) {
-    int s = lane < kZWarps ? scratch[lane] : 0;
-    int si = warp_incl_scan(s, lane);
-    if (lane < kZWarps) scratch[lane] = si - s;
-    if (lane == kZWarps - 1) scratch[32] = si;
-  }
+  int w = lane < kZWarps ? scratch[lane] : 0;
+  int wi = warp_incl_scan(w, lane);
+  int before = __shfl_sync(0xffffffffu, wi - w, warp);
+  *total = __shfl_sync(0xffffffffu, wi, kZWarps - 1);
   __syncthreads();
-  int r = scratch[warp] + incl - v;
-  *total = scratch[32];
-  __syncthreads();
-  return r;
+  return before + incl - v;
 }
 
 struct EncodeShared {
-  uint8_t in[kChunk];
+  uint8_t in[kChunk + 16];
   // payload staging: nonzero bytes (< osize) plus up to 2048 + 256 + 32 + 6
   // bitmap bytes before the size check can reject the encoding
-  uint8_t out[kChunk + 2048 + 512];
+  uint8_t out[kChunk + 2048 + 512 + 16];
   uint8_t bm0[2048];
   uint8_t bm1[256];
   uint8_t bm2[32];
@@ -96,6 +92,7 @@ struct EncodeShared {
   int scratch[40];
   long long ticket;
   long long excl;
+  int csz;
 };
 
 // repetition elimination of `n` (<= 2048) bitmap bytes held in shared memory:
@@ -134,14 +131,41 @@ __device__ __forceinline__ int re_encode_block(const uint8_t* bm, int n, uint8_t
   return total;
 }
 
-__global__ void __launch_bounds__(kZThreads)
+// Copy n bytes from shared memory to an arbitrarily aligned global address:
+// head bytes, then aligned 32-bit words (each assembled from two aligned
+// shared words), then the tail.
+__device__ __forceinline__ void copy_out(uint8_t* dst, const uint8_t* src, int n) {
+  const int tid = threadIdx.x;
+  int head = (int)((4 - ((uintptr_t)dst & 3)) & 3);
+  if (head > n) head = n;
+  if (tid < head) dst[tid] = src[tid];
+  const int words = (n - head) >> 2;
+  uint32_t* dw = reinterpret_cast<uint32_t*>(dst + head);
+  const int sh = head & 3;
+  const uint32_t* sw = reinterpret_cast<const uint32_t*>(src);
+  for (int w = tid; w < words; w += kZThreads) {
+    if (sh == 0) {
+      dw[w] = sw[w];
+    } else {
+      // bytes head + 4w .. +3 = words w and w+1 shifted by sh bytes
+      uint32_t lo = sw[w], hi = sw[w + 1];
+      dw[w] = __funnelshift_r(lo, hi, 8 * sh);
+    }
+  }
+  const int done = head + 4 * words;
+  if (tid < n - done) dst[done + tid] = src[done + tid];
+}
+
+// Persistent encoder: one CTA (512 threads, 32 bytes each) per 16 KiB chunk,
+// four CTAs per SM.
+__global__ void __launch_bounds__(kZThreads, 4)
 zbpc_encode_kernel(const uint8_t* __restrict__ planes, Geometry g, uint8_t* __restrict__ stream,
                    unsigned long long* __restrict__ status, unsigned long long* __restrict__ ticket,
                    uint64_t* __restrict__ comp_size_bp, uint64_t* __restrict__ lossless_size,
                    int* __restrict__ error_flag, long long spin_limit) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   EncodeShared& sh = *reinterpret_cast<EncodeShared*>(smem_raw);
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int64_t chunks = g.chunks;
   uint16_t* sizes = reinterpret_cast<uint16_t*>(stream + 8);
   uint8_t* data_out = stream + 8 + 2 * chunks;
@@ -150,38 +174,35 @@ zbpc_encode_kernel(const uint8_t* __restrict__ planes, Geometry g, uint8_t* __re
     __syncthreads();
     const int64_t id = sh.ticket;
     if (id >= chunks) break;
-    ChunkLoc loc = locate_chunk(g, id);
+    const ChunkLoc loc = locate_chunk(g, id);
     const int osize = loc.osize;
-    // load (base and osize are multiples of 8)
-    const uint2* src = reinterpret_cast<const uint2*>(planes + loc.base);
-    uint2* dst = reinterpret_cast<uint2*>(sh.in);
-    for (int i = tid; i < osize / 8; i += kZThreads) dst[i] = __ldg(src + i);
-    __syncthreads();
-    // zero elimination: each thread 32 bytes -> one 32-bit bitmap word
-    uint32_t bits = 0;
-    int b0 = tid * 32;
-    if (b0 < osize) {
-      const uint4* w = reinterpret_cast<const uint4*>(sh.in + b0);
+    // ---- load 32 bytes per thread (base and osize are multiples of 8) ----
+    const int b0 = tid * 32;
+    uint32_t wds[8];
+    {
+      const uint2* src = reinterpret_cast<const uint2*>(planes + loc.base + b0);
 #pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        uint4 v = w[q];
-        uint32_t words[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-        for (int k = 0; k < 4; ++k)
-#pragma unroll
-          for (int j = 0; j < 4; ++j)
-            bits |= (uint32_t)(((words[k] >> (8 * j)) & 0xFF) != 0) << (q * 16 + k * 4 + j);
+      for (int q = 0; q < 4; ++q) {
+        uint2 v = make_uint2(0, 0);
+        if (b0 + 8 * q < osize) v = __ldg(src + q);
+        wds[2 * q] = v.x;
+        wds[2 * q + 1] = v.y;
       }
-      if (b0 + 32 > osize) bits &= (1u << (osize - b0)) - 1u;
     }
-    reinterpret_cast<uint32_t*>(sh.bm0)[tid] = bits;  // 512 words = 2048 bytes
+    uint4* in4 = reinterpret_cast<uint4*>(sh.in + b0);
+    in4[0] = make_uint4(wds[0], wds[1], wds[2], wds[3]);
+    in4[1] = make_uint4(wds[4], wds[5], wds[6], wds[7]);
+    // zero elimination bitmap: bit j = byte b0 + j is nonzero
+    uint32_t bits = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) bits |= (uint32_t)(((wds[k] >> (8 * j)) & 0xFF) != 0) << (4 * k + j);
+    if (b0 + 32 > osize) bits = b0 >= osize ? 0u : bits & ((1u << (osize - b0)) - 1u);
+    reinterpret_cast<uint32_t*>(sh.bm0)[tid] = bits;
     int nz_total;
-    int off = block_excl_scan(__popc(bits), sh.scratch, &nz_total);
-    for (uint32_t m = bits; m; m &= m - 1) {
-      int j = __ffs(m) - 1;
-      sh.out[off++] = sh.in[b0 + j];
-    }
-    __syncthreads();
+    const int zoff = block_excl_scan(__popc(bits), sh.scratch, &nz_total);
+    // ---- decide the encoding; build the payload in sh.out ----
     int csize;
     bool raw = false;
     if (nz_total == 0) {
@@ -191,37 +212,93 @@ zbpc_encode_kernel(const uint8_t* __restrict__ planes, Geometry g, uint8_t* __re
       raw = true;
       csize = osize;
     } else {
-      int pos = nz_total;
-      int c1 = re_encode_block(sh.bm0, 2048, sh.out, pos, sh.bm1, sh.scratch);
-      pos += c1;
-      if (pos + 6 >= osize) { raw = true; csize = osize; }
-      else {
-        int c2 = re_encode_block(sh.bm1, 256, sh.out, pos, sh.bm2, sh.scratch);
-        pos += c2;
-        int c3 = re_encode_block(sh.bm2, 32, sh.out, pos, sh.bm3, sh.scratch);
-        pos += c3;
-        csize = pos + 6;
-        if (csize >= osize) { raw = true; csize = osize; }
-        else if (tid < 4) {
-          sh.out[pos + tid] = sh.bm3[tid];
-          if (tid == 0) { sh.out[pos + 4] = (uint8_t)osize; sh.out[pos + 5] = (uint8_t)(osize >> 8); }
+      // nonzero bytes, in order: every thread walks its 32 positions
+      {
+        int r = zoff;
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+          if ((bits >> j) & 1u) sh.out[r] = (uint8_t)(wds[j >> 2] >> (8 * (j & 3)));
+          r += (bits >> j) & 1u;
         }
       }
+      // RE 2048 -> 256: thread t flags bitmap bytes 4t..4t+3 (bm0 is complete
+      // since the scan's barriers)
+      const uint32_t cur = bits;
+      const uint32_t prev_byte = tid == 0 ? 0u : (reinterpret_cast<const uint32_t*>(sh.bm0)[tid - 1] >> 24);
+      uint32_t f1 = 0;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        uint32_t byte = (cur >> (8 * k)) & 0xFF;
+        uint32_t before = k == 0 ? prev_byte : ((cur >> (8 * (k - 1))) & 0xFF);
+        f1 |= (uint32_t)(byte != before) << k;
+      }
+      int c1;
+      const int r1 = block_excl_scan(__popc(f1), sh.scratch, &c1);
+      if (nz_total + c1 + 6 >= osize) {
+        raw = true;
+        csize = osize;
+      } else {
+        {
+          int r = nz_total + r1;
+#pragma unroll
+          for (int k = 0; k < 4; ++k)
+            if ((f1 >> k) & 1u) sh.out[r++] = (uint8_t)(cur >> (8 * k));
+        }
+        uint32_t other = __shfl_down_sync(0xffffffffu, f1, 1);
+        if ((tid & 1) == 0) sh.bm1[tid >> 1] = (uint8_t)(f1 | (other << 4));
+        __syncthreads();
+        if (warp == 0) {
+          // RE 256 -> 32: lane l flags bm1 bytes 8l..8l+7
+          uint32_t f2 = 0;
+          uint8_t b1[8];
+#pragma unroll
+          for (int k = 0; k < 8; ++k) b1[k] = sh.bm1[8 * lane + k];
+          uint8_t before = lane == 0 ? 0 : sh.bm1[8 * lane - 1];
+#pragma unroll
+          for (int k = 0; k < 8; ++k) {
+            f2 |= (uint32_t)(b1[k] != before) << k;
+            before = b1[k];
+          }
+          int cnt2 = __popc(f2);
+          int incl2 = warp_incl_scan(cnt2, lane);
+          int c2 = __shfl_sync(0xffffffffu, incl2, 31);
+          int r = nz_total + c1 + incl2 - cnt2;
+#pragma unroll
+          for (int k = 0; k < 8; ++k)
+            if ((f2 >> k) & 1u) sh.out[r++] = b1[k];
+          // RE 32 -> 4: lane l flags bm2 byte l (= f2)
+          uint32_t prev2 = __shfl_up_sync(0xffffffffu, f2, 1);
+          if (lane == 0) prev2 = 0;
+          uint32_t bal = __ballot_sync(0xffffffffu, f2 != prev2);
+          int c3 = __popc(bal);
+          int pos = nz_total + c1 + c2;
+          if ((f2 != prev2)) sh.out[pos + __popc(bal & ((1u << lane) - 1u))] = (uint8_t)f2;
+          pos += c3;
+          int cs = pos + 6;
+          if (lane == 0) sh.csz = cs;
+          if (cs < osize) {
+            if (lane < 4) sh.out[pos + lane] = (uint8_t)(bal >> (8 * lane));
+            if (lane == 0) { sh.out[pos + 4] = (uint8_t)osize; sh.out[pos + 5] = (uint8_t)(osize >> 8); }
+          }
+        }
+        __syncthreads();
+        csize = sh.csz;
+        if (csize >= osize) { raw = true; csize = osize; }
+      }
     }
-    __syncthreads();
-    // decoupled look-back: flag 1 = local size, flag 2 = inclusive prefix
-    if (tid < 32) {
+    // ---- decoupled look-back: flag 1 = local size, flag 2 = inclusive prefix ----
+    if (warp == 0) {
       const unsigned long long kAgg = 1ull << 62, kInc = 2ull << 62, kMask = (1ull << 62) - 1;
       if (id == 0) {
-        if (tid == 0) { atomicExch(&status[0], kInc | (unsigned long long)csize); sh.excl = 0; }
+        if (lane == 0) { atomicExch(&status[0], kInc | (unsigned long long)csize); sh.excl = 0; }
       } else {
-        if (tid == 0) atomicExch(&status[id], kAgg | (unsigned long long)csize);
+        if (lane == 0) atomicExch(&status[id], kAgg | (unsigned long long)csize);
         long long excl = 0;
         int64_t j = id - 1;
         long long spins = 0;
         bool done = false;
         while (!done) {
-          int64_t k = j - tid;
+          int64_t k = j - lane;
           unsigned long long v = k >= 0 ? 0ull : kInc;
           if (k >= 0) {
             do {
@@ -234,14 +311,14 @@ zbpc_encode_kernel(const uint8_t* __restrict__ planes, Geometry g, uint8_t* __re
           }
           unsigned inc_mask = __ballot_sync(0xffffffffu, (v >> 62) == 2);
           int stop = inc_mask ? __ffs(inc_mask) - 1 : 32;
-          long long part = (tid <= stop && tid < 32) ? (long long)(v & kMask) : 0;
+          long long part = lane <= stop ? (long long)(v & kMask) : 0;
 #pragma unroll
           for (int d = 16; d > 0; d >>= 1) part += __shfl_xor_sync(0xffffffffu, part, d);
           excl += part;
           if (inc_mask) done = true;
           else j -= 32;
         }
-        if (tid == 0) {
+        if (lane == 0) {
           atomicExch(&status[id], kInc | (unsigned long long)(excl + csize));
           sh.excl = excl;
         }
@@ -254,9 +331,7 @@ zbpc_encode_kernel(const uint8_t* __restrict__ planes, Geometry g, uint8_t* __re
       if (loc.last_of_plane) comp_size_bp[(3 - loc.level) * 32 + loc.plane] = (uint64_t)(offs + csize);
       if (id == chunks - 1) *lossless_size = (uint64_t)(offs + csize);
     }
-    const uint8_t* payload = raw ? sh.in : sh.out;
-    uint8_t* o = data_out + offs;
-    for (int i = tid; i < csize; i += kZThreads) o[i] = payload[i];
+    copy_out(data_out + offs, raw ? sh.in : sh.out, csize);
     __syncthreads();
   }
 }
@@ -328,57 +403,46 @@ __global__ void scan_add(int64_t* offs, int64_t n, const int64_t* block_sum) {
 }
 
 struct DecodeShared {
-  uint8_t in[kChunk + 16];
+  uint8_t in[kChunk + 32];
   uint8_t bm0[2048];
   uint8_t bm1[256];
   uint8_t bm2[32];
-  uint8_t bm3[4];
   int scratch[40];
+  int flag;
 };
 
-// fill-forward decode of `n` bitmap bytes from `data` with flags `bm`:
-// out[i] = data[rank(i) - 1] (0 when no flag yet), rank = inclusive popcount
-__device__ __forceinline__ void re_decode_block(const uint8_t* data, const uint8_t* bm, int n, uint8_t* out,
-                                                int* scratch) {
-  int per = n > kZThreads ? 4 : 1;
-  int i0 = threadIdx.x * per;
-  int flags = 0;
-  if (i0 < n)
-    for (int k = 0; k < per; ++k) flags |= ((bm[(i0 + k) >> 3] >> ((i0 + k) & 7)) & 1) << k;
-  int total;
-  int rank = block_excl_scan(__popc(flags), scratch, &total);
-  if (i0 < n) {
-    for (int k = 0; k < per; ++k) {
-      rank += (flags >> k) & 1;
-      out[i0 + k] = rank > 0 ? data[rank - 1] : 0;
-    }
+// Copy n bytes from an arbitrarily aligned global address into shared memory
+// with aligned 32-bit loads; no byte past src + n - 1's word is read.
+__device__ __forceinline__ void copy_in(uint8_t* dst, const uint8_t* src, int n) {
+  const int shift = (int)((uintptr_t)src & 3);
+  const uint32_t* a = reinterpret_cast<const uint32_t*>(src - shift);
+  const int last = (shift + n - 1) >> 2;  // last source word needed
+  uint32_t* dw = reinterpret_cast<uint32_t*>(dst);
+  for (int w = threadIdx.x; 4 * w < n; w += kZThreads) {
+    uint32_t lo = __ldg(a + w);
+    uint32_t hi = w + 1 <= last ? __ldg(a + w + 1) : 0u;
+    dw[w] = shift ? __funnelshift_r(lo, hi, 8 * shift) : lo;
   }
-  __syncthreads();
-}
-
-__device__ __forceinline__ int popc_bytes_block(const uint8_t* b, int n, int* scratch) {
-  int v = 0;
-  for (int i = threadIdx.x; i < n; i += kZThreads) v += __popc(b[i]);
-  int total;
-  block_excl_scan(v, scratch, &total);
-  return total;
 }
 
 // One CTA per chunk.  begin/end (device, may be null) select the chunks of
 // host planes [begin[3-l], end[3-l]) like zbpc_decode_progressive
-// (zbpc.cu:420-423).  Returns per-chunk errors through error_flag.
+// (zbpc.cu:420-423).  Corrupt chunks raise error_flag = 2.  The payload is
+// decoded from its tail: bitmap 4 B -> 32 B -> 256 B -> 2048 B (fill-forward:
+// byte i = kept byte rank(i) - 1, rank the inclusive flag count), then the
+// nonzero bytes are scattered by the zero-elimination bitmap.
 __global__ void __launch_bounds__(kZThreads)
 zbpc_decode_kernel(const uint8_t* __restrict__ stream, uint64_t stream_bytes, const int64_t* __restrict__ offs,
                    Geometry g, uint8_t* __restrict__ planes, const int* __restrict__ begin,
                    const int* __restrict__ end, int* __restrict__ error_flag) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   DecodeShared& sh = *reinterpret_cast<DecodeShared*>(smem_raw);
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int64_t chunks = g.chunks;
   const uint16_t* sizes = reinterpret_cast<const uint16_t*>(stream + 8);
   const uint8_t* data_in = stream + 8 + 2 * chunks;
   for (int64_t id = blockIdx.x; id < chunks; id += gridDim.x) {
-    ChunkLoc loc = locate_chunk(g, id);
+    const ChunkLoc loc = locate_chunk(g, id);
     if (begin) {
       int64_t cpp = g.chunks_level[loc.level] >> 5;
       int64_t real = loc.plane * cpp + loc.offset;
@@ -393,51 +457,93 @@ zbpc_decode_kernel(const uint8_t* __restrict__ stream, uint64_t stream_bytes, co
     }
     const uint8_t* src = data_in + offs[id];
     uint8_t* dst = planes + loc.base;
-    if (csize == osize) {  // raw chunk
-      for (int i = tid; i < osize; i += kZThreads) dst[i] = src[i];
-      continue;
-    }
-    for (int i = tid; i < csize; i += kZThreads) sh.in[i] = src[i];
-    __syncthreads();
-    bool bad = csize < 2 || (sh.in[csize - 2] | (sh.in[csize - 1] << 8)) != osize;
-    int rpos = csize - 2;
-    if (!bad && rpos == 0) {  // all zero
-      uint2* d2 = reinterpret_cast<uint2*>(dst);
-      for (int i = tid; i < osize / 8; i += kZThreads) d2[i] = make_uint2(0, 0);
+    const int b0 = tid * 32;
+    if (csize == osize) {  // raw chunk: 32 bytes per thread through shared memory
+      copy_in(sh.in, src, osize);
+      __syncthreads();
+      if (b0 < osize) {
+        const uint2* s2 = reinterpret_cast<const uint2*>(sh.in + b0);
+        uint2* d2 = reinterpret_cast<uint2*>(dst + b0);
+        const int nq = min(4, (osize - b0) >> 3);
+        for (int q = 0; q < nq; ++q) d2[q] = s2[q];
+      }
       __syncthreads();
       continue;
     }
-    if (!bad && rpos < 4) bad = true;
+    copy_in(sh.in, src, csize);
+    if (tid == 0) sh.flag = 0;
+    __syncthreads();
+    bool bad = csize < 2 || (sh.in[csize - 2] | (sh.in[csize - 1] << 8)) != osize;
+    if (!bad && csize == 2) {  // all zero
+      if (b0 < osize) {
+        uint2* d2 = reinterpret_cast<uint2*>(dst + b0);
+        const int nq = min(4, (osize - b0) >> 3);
+        for (int q = 0; q < nq; ++q) d2[q] = make_uint2(0, 0);
+      }
+      __syncthreads();
+      continue;
+    }
+    if (!bad && csize < 6) bad = true;
     if (bad) {
       if (tid == 0) atomicExch(error_flag, 2);
       __syncthreads();
       continue;
     }
-    rpos -= 4;
-    if (tid < 4) sh.bm3[tid] = sh.in[rpos + tid];
+    // ---- warp 0: bm3 (4 B) -> bm2 (32 B) -> bm1 (256 B) ----
+    int rpos = csize - 6;  // start of bm3
+    if (warp == 0) {
+      const uint32_t bm3 = (uint32_t)sh.in[rpos] | ((uint32_t)sh.in[rpos + 1] << 8) |
+                           ((uint32_t)sh.in[rpos + 2] << 16) | ((uint32_t)sh.in[rpos + 3] << 24);
+      const int c3 = __popc(bm3);
+      const int p3 = rpos - c3;  // RE3 bytes
+      // bm2 byte l = kept byte (inclusive rank of flag l) - 1, or 0
+      const int rank3 = __popc(bm3 & (0xffffffffu >> (31 - lane)));
+      uint32_t b2 = 0;
+      if (p3 >= 0 && rank3 > 0) b2 = sh.in[p3 + rank3 - 1];
+      sh.bm2[lane] = (uint8_t)b2;
+      // bm2 flags 256 bits: lane l owns flags 8l..8l+7 = byte b2 of lane l
+      const int cnt2 = __popc(b2);
+      const int incl2 = warp_incl_scan(cnt2, lane);
+      const int c2 = __shfl_sync(0xffffffffu, incl2, 31);
+      const int p2 = p3 - c2;  // RE2 bytes
+      int r = incl2 - cnt2;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        r += (b2 >> k) & 1u;
+        sh.bm1[8 * lane + k] = (p2 >= 0 && r > 0) ? sh.in[p2 + r - 1] : 0;
+      }
+      if (lane == 0) {
+        sh.scratch[36] = p2;
+        if (p3 < 0 || p2 < 0) sh.flag = 1;
+      }
+    }
     __syncthreads();
-    int c3 = popc_bytes_block(sh.bm3, 4, sh.scratch);
-    rpos -= c3;
-    bool ok = rpos >= 0;
-    if (ok) re_decode_block(sh.in + rpos, sh.bm3, 32, sh.bm2, sh.scratch);
-    int c2 = ok ? popc_bytes_block(sh.bm2, 32, sh.scratch) : 0;
-    rpos -= c2;
-    ok = ok && rpos >= 0;
-    if (ok) re_decode_block(sh.in + rpos, sh.bm2, 256, sh.bm1, sh.scratch);
-    int c1 = ok ? popc_bytes_block(sh.bm1, 256, sh.scratch) : 0;
-    rpos -= c1;
-    ok = ok && rpos >= 0;
-    if (ok) re_decode_block(sh.in + rpos, sh.bm1, 2048, sh.bm0, sh.scratch);
-    if (!ok) {
+    const int p2 = sh.scratch[36];
+    if (sh.flag) {
       if (tid == 0) atomicExch(error_flag, 2);
       __syncthreads();
       continue;
     }
-    // zero-elimination decode: thread t owns bytes [32t, 32t+32)
-    uint32_t bits = reinterpret_cast<const uint32_t*>(sh.bm0)[tid];
-    int b0 = tid * 32;
-    int total;
-    int rank = block_excl_scan(__popc(bits), sh.scratch, &total);
+    // ---- all threads: bm1 (2048 flags) -> bm0 (2048 B); thread t owns bm0 bytes 4t..4t+3 ----
+    const uint32_t f1 = (sh.bm1[tid >> 1] >> (4 * (tid & 1))) & 0xFu;
+    int c1;
+    int r1 = block_excl_scan(__popc(f1), sh.scratch, &c1);
+    const int p1 = p2 - c1;  // RE1 bytes
+    if (p1 < 0) {
+      if (tid == 0) atomicExch(error_flag, 2);
+      __syncthreads();
+      continue;
+    }
+    // fill-forward: byte i = RE1 byte (rank(i) - 1), rank inclusive; rank 0 -> 0
+    uint32_t bits = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      r1 += (f1 >> k) & 1u;
+      bits |= (uint32_t)(r1 > 0 ? sh.in[p1 + r1 - 1] : 0) << (8 * k);
+    }
+    // bits = this thread's 32 zero-elimination flags (bytes b0 .. b0+31)
+    int nz;
+    int rank = block_excl_scan(__popc(bits), sh.scratch, &nz);
     if (b0 < osize) {
       uint32_t w[8];
 #pragma unroll
@@ -445,23 +551,17 @@ zbpc_decode_kernel(const uint8_t* __restrict__ stream, uint64_t stream_bytes, co
         uint32_t v = 0;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-          int bit = q * 4 + j;
-          uint32_t byte = 0;
-          if ((bits >> bit) & 1) byte = sh.in[rank++];
-          v |= byte << (8 * j);
+          const int bit = q * 4 + j;
+          if ((bits >> bit) & 1u) v |= (uint32_t)sh.in[rank] << (8 * j);
+          rank += (bits >> bit) & 1u;
         }
         w[q] = v;
       }
-      int nb = osize - b0 < 32 ? osize - b0 : 32;
-      if (nb == 32) {
-        uint2* d2 = reinterpret_cast<uint2*>(dst + b0);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) d2[q] = make_uint2(w[2 * q], w[2 * q + 1]);
-      } else {
-        for (int b = 0; b < nb; ++b) dst[b0 + b] = (uint8_t)(w[b >> 2] >> (8 * (b & 3)));
-      }
+      uint2* d2 = reinterpret_cast<uint2*>(dst + b0);
+      const int nq = min(4, (osize - b0) >> 3);
+      for (int q = 0; q < nq; ++q) d2[q] = make_uint2(w[2 * q], w[2 * q + 1]);
     }
-    if (total > rpos && tid == 0) atomicExch(error_flag, 2);
+    if (nz > p1 && tid == 0) atomicExch(error_flag, 2);
     __syncthreads();
   }
 }
