@@ -59,6 +59,7 @@ class ClockSampler:
         self.index = index
         self.proc = None
         self.path = None
+        self.skip = 0
 
     def start(self):
         fd, self.path = tempfile.mkstemp(suffix=".csv")
@@ -68,10 +69,16 @@ class ClockSampler:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "20"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        # wait for the first sample so that the timed region is covered
+        t0 = time.time()
+        while time.time() - t0 < 3.0 and os.path.getsize(self.path) == 0:
+            time.sleep(0.01)
+        self.skip = sum(1 for _ in open(self.path))
 
     def stop(self):
         if not self.proc:
@@ -83,7 +90,11 @@ class ClockSampler:
             self.proc.kill()
         sm, mx, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
+        lines = open(self.path).read().splitlines()
+        # samples taken before the timed region started are dropped, unless
+        # the region was shorter than one sampling interval
+        lines = lines[self.skip:] or lines[-1:]
+        for line in lines:
             f = [x.strip() for x in line.split(",")]
             if len(f) < 9:
                 continue

@@ -183,6 +183,78 @@ int prism_lossless_encode_static(const uint8_t* d_planes, uint32_t nx, uint32_t 
 int prism_find_strategy(prism_handle* h, const uint64_t comp_size_bp[128], double eb,
                         double target_error, int begin[4], int end[4], int* maxlevel, void* stream);
 
+/* ---- batched compression ----------------------------------------------
+ * Many fields of uneven shapes compressed by one launch per pipeline stage;
+ * no counterpart in the reference, whose pipeline handles one field per call
+ * (Compressor<T,i4>::compress_pipeline, src/compressor.cu:120-151).  Every
+ * field's container is byte-identical to prism_compress of that field. */
+typedef struct prism_field_desc {
+  const void* d_in;       /* device input, nx*ny*nz values, x fastest */
+  void* d_out;            /* device container buffer */
+  uint64_t out_capacity;  /* >= prism_max_container_size of the field */
+  uint32_t nx, ny, nz;
+  int dtype_size;         /* 4 or 8 */
+  int mode;               /* 0 ABS, 1 REL */
+  double bound;
+  int progressive;        /* 0 sign-magnitude planes, 1 negabinary */
+} prism_field_desc;
+
+typedef struct prism_batch prism_batch;
+
+/* Plan a batch for these fields and buffers: one device workspace for all
+ * fields, work tables per stage, a schedule tuned on the batch itself (CTAs
+ * per SM of the persistent predictor and encoder, timed on the first runs),
+ * and, when use_graph != 0, the whole pipeline captured in a CUDA graph.
+ * Runs the pipeline a few times while tuning, on the current device. */
+int prism_batch_create(const prism_field_desc* fields, int n, int use_graph, prism_batch** out);
+/* Compress the current contents of the batch's input buffers into its output
+ * buffers; sizes_out[i] receives field i's container size and flags_out
+ * (may be NULL) its use_md[4], reverse[4].  Waits for `stream`. */
+int prism_batch_compress(prism_batch* b, void* stream, uint64_t* sizes_out, uint8_t* flags_out);
+/* The tuned schedule: predictor CTAs per SM for float and double fields,
+ * encoder CTAs per SM, the tuned stage times (ms) and kernels per run. */
+int prism_batch_schedule(const prism_batch* b, int pred_ctas_per_sm[2], int* enc_ctas_per_sm, double tuned_ms[2],
+                         uint64_t* launches_per_run);
+const char* prism_batch_last_error(const prism_batch* b);
+void prism_batch_destroy(prism_batch* b);
+
+/* ---- progressive-retrieval server -----------------------------------------
+ * No counterpart in the reference, whose CLI reloads and re-decodes the whole
+ * container for each -errors target (src/prism.cu:131-190).  The server keeps
+ * -prog containers and reconstructions resident on the current device and
+ * answers "field f at error bound t" requests from `slots` worker threads
+ * (one stream and workspace each) under an HBM budget.  A request's values are
+ * those of a one-step progressive retrieval of f to t (prism_progressive_open
+ * + one prism_progressive_step), whatever else is in flight; reconstructions
+ * are cached per selected plane set and reused bit for bit. */
+typedef struct prism_server prism_server;
+typedef struct prism_server_stats {
+  uint64_t completed, cache_hits, shared, evictions, failed;
+  uint64_t bytes_out, bytes_resident, bytes_reserved, bytes_peak;
+  double p50_ms, p99_ms, mean_ms, max_ms, elapsed_s;
+} prism_server_stats;
+
+/* hbm_budget: bytes of device memory the server may hold (containers,
+ * cached reconstructions, per-slot workspaces). */
+int prism_server_create(uint64_t hbm_budget, int slots, prism_server** out);
+/* Copy a -prog container (host, or device when on_device != 0) into the
+ * server; *field_id names it in requests.  PRISM_ERR_NOMEM beyond the budget. */
+int prism_server_add_field(prism_server* s, const void* container, uint64_t size, int on_device, int dtype_size,
+                           uint32_t nx, uint32_t ny, uint32_t nz, int mode, double bound, int* field_id);
+/* Queue a retrieval of field_id at target_error (the same kind of bound as
+ * the field's mode) into `out` (nx*ny*nz values; device memory when
+ * out_on_device != 0, else host memory).  Returns at once. */
+int prism_server_submit(prism_server* s, int field_id, double target_error, void* out, int out_on_device,
+                        uint64_t* request_id);
+/* Wait for a request; latency = submit to completion.  end/maxlevel receive
+ * the plane selection, from_cache whether a resident reconstruction served it.
+ * Returns the request's status. */
+int prism_server_wait(prism_server* s, uint64_t request_id, double* latency_ms, int end[4], int* maxlevel,
+                      int* from_cache);
+/* Latency percentiles and counters of the completed requests. */
+int prism_server_stats_get(prism_server* s, prism_server_stats* out, int reset);
+void prism_server_destroy(prism_server* s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -74,6 +74,18 @@ def lib():
         l.prism_lossless_decode.argtypes = [vp, vp, u32, u32, u32, vp, vp, vp, vp]
         l.prism_find_strategy.argtypes = [vp, vp, dbl, dbl, vp, vp, vp, vp]
         l.prism_lossless_encode_static.argtypes = [vp, u32, u32, u32, vp, u64, C.POINTER(u64), vp, vp]
+        l.prism_batch_create.argtypes = [vp, i32, i32, C.POINTER(vp)]
+        l.prism_batch_compress.argtypes = [vp, vp, vp, vp]
+        l.prism_batch_schedule.argtypes = [vp, vp, vp, vp, vp]
+        l.prism_batch_last_error.argtypes = [vp]
+        l.prism_batch_last_error.restype = C.c_char_p
+        l.prism_batch_destroy.argtypes = [vp]
+        l.prism_server_create.argtypes = [u64, i32, C.POINTER(vp)]
+        l.prism_server_add_field.argtypes = [vp, vp, u64, i32, i32, u32, u32, u32, i32, dbl, C.POINTER(i32)]
+        l.prism_server_submit.argtypes = [vp, i32, dbl, vp, i32, C.POINTER(u64)]
+        l.prism_server_wait.argtypes = [vp, u64, C.POINTER(dbl), vp, C.POINTER(i32), C.POINTER(i32)]
+        l.prism_server_stats_get.argtypes = [vp, vp, i32]
+        l.prism_server_destroy.argtypes = [vp]
         l.prism_profile.argtypes = [vp, i32]
         l.prism_stage_times.argtypes = [vp, vp, vp, i32, i32]
         l.prism_launch_count.argtypes = [vp]
@@ -90,6 +102,9 @@ EXPORTED = [
     "prism_code_buffer_len", "prism_predict", "prism_reconstruct", "prism_bitshuffle",
     "prism_inverse_bitshuffle", "prism_lossless_encode", "prism_lossless_decode", "prism_find_strategy",
     "prism_profile", "prism_stage_times", "prism_launch_count", "prism_lossless_encode_static",
+    "prism_batch_create", "prism_batch_compress", "prism_batch_schedule", "prism_batch_last_error",
+    "prism_batch_destroy", "prism_server_create", "prism_server_add_field", "prism_server_submit",
+    "prism_server_wait", "prism_server_stats_get", "prism_server_destroy",
 ]
 
 STAGES = ["extrema", "autotune", "predict", "shuffle", "encode", "trailer", "strategy", "decode",
@@ -240,6 +255,139 @@ class Progressive:
     def close(self):
         if self.ptr:
             lib().prism_progressive_close(self.ptr)
+            self.ptr = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class FieldDesc(C.Structure):
+    """prism_field_desc: one field of a batch (device buffers)."""
+    _fields_ = [("d_in", C.c_void_p), ("d_out", C.c_void_p), ("out_capacity", C.c_uint64), ("nx", C.c_uint32),
+                ("ny", C.c_uint32), ("nz", C.c_uint32), ("dtype_size", C.c_int), ("mode", C.c_int),
+                ("bound", C.c_double), ("progressive", C.c_int)]
+
+
+class Batch:
+    """Batched compression of many fields (prism_batch_*): one launch per stage
+    over all fields, a schedule tuned on the batch, the pipeline captured in a
+    CUDA graph.  `items` is a list of (Context, device input tensor); output
+    buffers are allocated here and stay bound to the batch."""
+
+    def __init__(self, items, use_graph=True):
+        torch = _torch()
+        self.items = items
+        self.outs = []
+        descs = (FieldDesc * len(items))()
+        for i, (ctx, d_in) in enumerate(items):
+            cap = int(lib().prism_max_container_size(ctx.nx, ctx.ny, ctx.nz, ctx.tsize))
+            out = torch.empty(cap, dtype=torch.uint8, device=d_in.device)
+            self.outs.append(out)
+            descs[i] = FieldDesc(d_in.data_ptr(), out.data_ptr(), cap, ctx.nx, ctx.ny, ctx.nz, ctx.tsize,
+                                 ctx.error_mode, ctx.bound, int(ctx.progressive))
+        self.ptr = C.c_void_p()
+        rc = lib().prism_batch_create(descs, len(items), int(use_graph), C.byref(self.ptr))
+        if rc:
+            raise PrismError(f"prism_batch_create: {_STATUS.get(rc, rc)}")
+
+    def compress(self):
+        """Returns the list of containers (views into the bound outputs) and flags."""
+        torch = _torch()
+        n = len(self.items)
+        sizes = (C.c_uint64 * n)()
+        flags = (C.c_uint8 * (8 * n))()
+        rc = lib().prism_batch_compress(self.ptr, _stream(torch), sizes, flags)
+        if rc:
+            raise PrismError(f"prism_batch_compress: {_STATUS.get(rc, rc)}: "
+                             f"{lib().prism_batch_last_error(self.ptr).decode()}")
+        conts = [self.outs[i][: sizes[i]] for i in range(n)]
+        fl = [(tuple(flags[8 * i:8 * i + 4]), tuple(flags[8 * i + 4:8 * i + 8])) for i in range(n)]
+        return conts, fl
+
+    def schedule(self):
+        pred = (C.c_int * 2)()
+        enc = C.c_int()
+        ms = (C.c_double * 2)()
+        launches = C.c_uint64()
+        lib().prism_batch_schedule(self.ptr, pred, C.byref(enc), ms, C.byref(launches))
+        return {"predict_ctas_per_sm": list(pred), "encode_ctas_per_sm": enc.value,
+                "tuned_ms": list(ms), "launches_per_run": launches.value}
+
+    def close(self):
+        if self.ptr:
+            lib().prism_batch_destroy(self.ptr)
+            self.ptr = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(k, C.c_uint64) for k in ("completed", "cache_hits", "shared", "evictions", "failed", "bytes_out",
+                                          "bytes_resident", "bytes_reserved", "bytes_peak")] + \
+               [(k, C.c_double) for k in ("p50_ms", "p99_ms", "mean_ms", "max_ms", "elapsed_s")]
+
+
+class Server:
+    """Progressive-retrieval server (prism_server_*): -prog containers and
+    reconstructions resident on the device, requests served by `slots`
+    worker threads under an HBM budget (bytes)."""
+
+    def __init__(self, hbm_budget, slots=4):
+        self.ptr = C.c_void_p()
+        rc = lib().prism_server_create(int(hbm_budget), int(slots), C.byref(self.ptr))
+        if rc:
+            raise PrismError(f"prism_server_create: {_STATUS.get(rc, rc)}")
+        self.fields = []
+
+    def add_field(self, ctx: Context, container):
+        """container: uint8 CUDA tensor or numpy array of a -prog container."""
+        fid = C.c_int()
+        on_dev = hasattr(container, "is_cuda") and container.is_cuda
+        ptr = container.data_ptr() if on_dev else container.ctypes.data
+        n = container.numel() if on_dev else container.size
+        rc = lib().prism_server_add_field(self.ptr, C.c_void_p(ptr), n, int(on_dev), ctx.tsize, ctx.nx, ctx.ny,
+                                          ctx.nz, ctx.error_mode, ctx.bound, C.byref(fid))
+        if rc:
+            raise PrismError(f"prism_server_add_field: {_STATUS.get(rc, rc)}")
+        self.fields.append(ctx)
+        return fid.value
+
+    def submit(self, field_id, target, out):
+        """out: CUDA tensor (or numpy array) of the field's shape and dtype."""
+        rid = C.c_uint64()
+        on_dev = hasattr(out, "is_cuda") and out.is_cuda
+        ptr = out.data_ptr() if on_dev else out.ctypes.data
+        rc = lib().prism_server_submit(self.ptr, int(field_id), float(target), C.c_void_p(ptr), int(on_dev),
+                                       C.byref(rid))
+        if rc:
+            raise PrismError(f"prism_server_submit: {_STATUS.get(rc, rc)}")
+        return rid.value
+
+    def wait(self, request_id):
+        lat = C.c_double()
+        end = (C.c_int * 4)()
+        ml = C.c_int()
+        hit = C.c_int()
+        rc = lib().prism_server_wait(self.ptr, C.c_uint64(request_id), C.byref(lat), end, C.byref(ml), C.byref(hit))
+        if rc:
+            raise PrismError(f"prism_server_wait: {_STATUS.get(rc, rc)}")
+        return {"latency_ms": lat.value, "end": list(end), "maxlevel": ml.value, "from_cache": bool(hit.value)}
+
+    def stats(self, reset=False):
+        st = ServerStats()
+        lib().prism_server_stats_get(self.ptr, C.byref(st), int(reset))
+        return {k: getattr(st, k) for k, _ in ServerStats._fields_}
+
+    def close(self):
+        if self.ptr:
+            lib().prism_server_destroy(self.ptr)
             self.ptr = C.c_void_p()
 
     def __del__(self):

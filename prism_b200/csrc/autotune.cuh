@@ -141,11 +141,8 @@ __device__ T block_sum(T v, T* red) {
 // (pre_compute_att :111-141): 0 -> levels 3 and 2, 1-2 -> level 1
 // (2 = natural cubic), 3-5 -> level 0.  partial[window][15].
 template <class T>
-__global__ void __launch_bounds__(kAttThreads)
-autotune_kernel(const T* __restrict__ data, Geometry g, const SampleWindow* __restrict__ wins, T* __restrict__ partial) {
-  __shared__ T win[kWinVol];
-  __shared__ T red[kAttThreads];
-  SampleWindow w = wins[blockIdx.x];
+__device__ __forceinline__ void autotune_window(T* win, T* red, const T* __restrict__ data, const Geometry& g,
+                                                const SampleWindow w, int biy, T* out) {
   TileCtx<T> t;
   t.s = win;
   t.dim[0] = g.nx; t.dim[1] = g.ny; t.dim[2] = g.nz;
@@ -159,8 +156,6 @@ autotune_kernel(const T* __restrict__ data, Geometry g, const SampleWindow* __re
     win[i] = v;
   }
   __syncthreads();
-  T* out = partial + (size_t)blockIdx.x * 15;
-  int biy = blockIdx.y;
   if (biy == 0) {
     T e[6];
     e[0] = att_level(t, 3, false, false, false);
@@ -186,16 +181,24 @@ autotune_kernel(const T* __restrict__ data, Geometry g, const SampleWindow* __re
   }
 }
 
+template <class T>
+__global__ void __launch_bounds__(kAttThreads)
+autotune_kernel(const T* __restrict__ data, Geometry g, const SampleWindow* __restrict__ wins, T* __restrict__ partial) {
+  __shared__ T win[kWinVol];
+  __shared__ T red[kAttThreads];
+  autotune_window<T>(win, red, data, g, wins[blockIdx.x], blockIdx.y, partial + (size_t)blockIdx.x * 15);
+}
+
 // Field parameters, computed on the device so nothing waits for the host:
 // bound (ABS, or REL x range), calc_eb per level (:1825-1839) with the double
 // alpha/beta and, when `partial` is given, the auto-tune decisions (:2306-2355)
 // from the window sums.  Flags otherwise come from `flags_in` (a container).
 template <class T>
-__global__ void params_kernel(int mode, double bound, const double* __restrict__ range, double alpha,
-                              const T* __restrict__ partial, int nwin, const uint8_t* __restrict__ flags_in,
-                              int maxlevel, PredParams<T>* __restrict__ out, T* __restrict__ errors_out,
-                              double* __restrict__ eb_out) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__device__ __forceinline__ void compute_params(int mode, double bound, const double* __restrict__ range, double alpha,
+                                               const T* __restrict__ partial, int nwin,
+                                               const uint8_t* __restrict__ flags_in, int maxlevel,
+                                               PredParams<T>* __restrict__ out, T* __restrict__ errors_out,
+                                               double* __restrict__ eb_out) {
   using F = Fp<T>;
   PredParams<T> p;
   double eb = mode == 1 ? __dmul_rn(bound, *range) : bound;
@@ -244,6 +247,15 @@ __global__ void params_kernel(int mode, double bound, const double* __restrict__
   p.maxlevel = maxlevel;
   *out = p;
   if (eb_out) *eb_out = eb;
+}
+
+template <class T>
+__global__ void params_kernel(int mode, double bound, const double* __restrict__ range, double alpha,
+                              const T* __restrict__ partial, int nwin, const uint8_t* __restrict__ flags_in,
+                              int maxlevel, PredParams<T>* __restrict__ out, T* __restrict__ errors_out,
+                              double* __restrict__ eb_out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  compute_params<T>(mode, bound, range, alpha, partial, nwin, flags_in, maxlevel, out, errors_out, eb_out);
 }
 
 // Global min / max (compressor.cu:230-302): per-block partials, then one block.

@@ -94,13 +94,11 @@ __device__ __forceinline__ void locate_item(const ShufPlan& s, int64_t item, int
 // consecutive codes of one level: 32 coalesced 128-byte loads, 32 register
 // transposes, then through a padded shared-memory tile so that each plane's
 // 128 bytes leave as one contiguous warp store.
-__global__ void __launch_bounds__(kShufWarps * 32)
-bitshuffle_kernel(const int32_t* __restrict__ codes, uint8_t* __restrict__ planes, Geometry g,
-                  ShufPlan plan, int nb) {
-  __shared__ uint32_t tile[kShufWarps][32][33];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  int64_t item = (int64_t)blockIdx.x * kShufWarps + warp;
-  if (item >= plan.items) return;
+// One warp work item of the forward shuffle (tw: the warp's staging tile).
+__device__ __forceinline__ void shuffle_item(uint32_t (&tw)[32][33], const int32_t* __restrict__ codes,
+                                             uint8_t* __restrict__ planes, const Geometry& g, const ShufPlan& plan,
+                                             int nb, int64_t item) {
+  const int lane = threadIdx.x & 31;
   int level;
   int64_t local;
   locate_item(plan, item, &level, &local);
@@ -108,7 +106,6 @@ bitshuffle_kernel(const int32_t* __restrict__ codes, uint8_t* __restrict__ plane
   int64_t count = pick4(plan.proc, level) - first;
   if (count > kShufCodes) count = kShufCodes;
   const int32_t* src = codes + pick4(plan.seg_start, level) + first;
-  uint32_t (&tw)[32][33] = tile[warp];
   if (count == kShufCodes) {
     int32_t c[32];
 #pragma unroll
@@ -138,6 +135,15 @@ bitshuffle_kernel(const int32_t* __restrict__ codes, uint8_t* __restrict__ plane
       for (int b = 4 * lane; b < nbytes; ++b) dst[b] = (uint8_t)(w >> (8 * (b & 3)));
     }
   }
+}
+
+__global__ void __launch_bounds__(kShufWarps * 32)
+bitshuffle_kernel(const int32_t* __restrict__ codes, uint8_t* __restrict__ planes, Geometry g,
+                  ShufPlan plan, int nb) {
+  __shared__ uint32_t tile[kShufWarps][32][33];
+  int64_t item = (int64_t)blockIdx.x * kShufWarps + (threadIdx.x >> 5);
+  if (item >= plan.items) return;
+  shuffle_item(tile[threadIdx.x >> 5], codes, planes, g, plan, nb, item);
 }
 
 // planes -> codes; begin/end (device, may be null) restrict each level to
@@ -243,9 +249,8 @@ __device__ __forceinline__ int64_t place_dev(const Geometry& g, int64_t c, int64
   return (idx >> 3) + g.dstride[level] * ((idx & 7) << 2) + g.daprefix[level];
 }
 
-__global__ void __launch_bounds__(512)
-shuffle_last_block_kernel(const int32_t* __restrict__ codes, uint8_t* __restrict__ planes, Geometry g,
-                          int nb, uint64_t limit) {
+__device__ __forceinline__ void shuffle_last_block(const int32_t* __restrict__ codes, uint8_t* __restrict__ planes,
+                                                   const Geometry& g, int nb, uint64_t limit, int cta, int ncta) {
   __shared__ uint32_t a[512];
   __shared__ uint32_t shm[512];
   __shared__ unsigned char act[512];
@@ -257,7 +262,7 @@ shuffle_last_block_kernel(const int32_t* __restrict__ codes, uint8_t* __restrict
   shm[t] = 0;
   // a round only reads words its own round wrote; whether rounds may run in
   // parallel is decided by the launch (shuffle_last_block_grid)
-  for (int64_t base = (int64_t)blockIdx.x * 512; base < maxa; base += (int64_t)gridDim.x * 512) {
+  for (int64_t base = (int64_t)cta * 512; base < maxa; base += (int64_t)ncta * 512) {
     bool part = base < ares;
     bool ac = part && base + t < res;
     act[t] = ac;
@@ -286,6 +291,12 @@ shuffle_last_block_kernel(const int32_t* __restrict__ codes, uint8_t* __restrict
     }
     __syncthreads();
   }
+}
+
+__global__ void __launch_bounds__(512)
+shuffle_last_block_kernel(const int32_t* __restrict__ codes, uint8_t* __restrict__ planes, Geometry g,
+                          int nb, uint64_t limit) {
+  shuffle_last_block(codes, planes, g, nb, limit, blockIdx.x, gridDim.x);
 }
 
 // inverse of the last block (bitplane.cu:400-450 and :532-600): thread t

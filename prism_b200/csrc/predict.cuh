@@ -270,7 +270,7 @@ struct AxisLimits {
 
 template <bool EDGE>
 struct Limits {
-  const AxisLimits& a;
+  AxisLimits a;  // by value: stays in registers
   __device__ __forceinline__ int l3(int d) const { return EDGE ? a.l3[d] : 16; }
   __device__ __forceinline__ int l1(int d) const { return EDGE ? a.l1[d] : 1 << 20; }
   __device__ __forceinline__ int r(int d) const { return EDGE ? a.r[d] : kWin; }
@@ -493,8 +493,7 @@ PRISM_HD uint64_t tiles_in_part(const Geometry& g, int part) {
 }
 
 template <int PART>
-__device__ __forceinline__ void tile_of_block(const Geometry& g, uint32_t bi[3]) {
-  uint32_t j = blockIdx.x;
+__device__ __forceinline__ void tile_of_index(const Geometry& g, uint32_t j, uint32_t bi[3]) {
   if (PART == 0) {
     bi[0] = j % (g.ax - 1); bi[1] = (j / (g.ax - 1)) % (g.ay - 1); bi[2] = j / ((g.ax - 1) * (g.ay - 1));
     return;
@@ -504,6 +503,11 @@ __device__ __forceinline__ void tile_of_block(const Geometry& g, uint32_t bi[3])
   if (j < g.ax * (g.az - 1)) { bi[0] = j % g.ax; bi[1] = g.ay - 1; bi[2] = j / g.ax; return; }
   j -= g.ax * (g.az - 1);
   bi[0] = g.ax - 1; bi[1] = j % (g.ay - 1); bi[2] = j / (g.ay - 1);
+}
+
+template <int PART>
+__device__ __forceinline__ void tile_of_block(const Geometry& g, uint32_t bi[3]) {
+  tile_of_index<PART>(g, blockIdx.x, bi);
 }
 
 // Per-tile frame: window origin, limits, and the level-0 slot of each window
@@ -592,15 +596,13 @@ struct ReconSmem {
 // The window is loaded with kPrefetch independent loads per thread in flight,
 // the 12 stages run in shared memory, and the codes of the points the tile
 // owns leave in one pass at the end.
-template <class T, int PART>
-__global__ void __launch_bounds__(kPredThreads)
-predict_compress_kernel(const T* __restrict__ data, Geometry g, const PredParams<T>* __restrict__ pp,
-                        T* __restrict__ anchors, int32_t* __restrict__ qc) {
-  constexpr bool EDGE = PART == 1;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  CompressSmem<T>& sm = *reinterpret_cast<CompressSmem<T>*>(smem_raw);
-  uint32_t bi[3];
-  tile_of_block<PART>(g, bi);
+// One tile of the compression (the body of predict_compress_kernel and of the
+// batched persistent kernel).  The caller guarantees that no thread still
+// reads `sm` from a previous tile.
+template <class T, bool EDGE>
+__device__ __forceinline__ void compress_tile(CompressSmem<T>& sm, const T* __restrict__ data, const Geometry& g,
+                                              const uint32_t bi[3], const PredParams<T>* __restrict__ pp,
+                                              T* __restrict__ anchors, int32_t* __restrict__ qc) {
   TileFrame f;
   tile_frame(g, bi, f);
   const Limits<EDGE> L{f.lim};
@@ -637,12 +639,23 @@ predict_compress_kernel(const T* __restrict__ data, Geometry g, const PredParams
   }
 }
 
+template <class T, int PART>
+__global__ void __launch_bounds__(kPredThreads, 3)
+predict_compress_kernel(const T* __restrict__ data, Geometry g, const PredParams<T>* __restrict__ pp,
+                        T* __restrict__ anchors, int32_t* __restrict__ qc) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  CompressSmem<T>& sm = *reinterpret_cast<CompressSmem<T>*>(smem_raw);
+  uint32_t bi[3];
+  tile_of_block<PART>(g, bi);
+  compress_tile<T, PART == 1>(sm, data, g, bi, pp, anchors, qc);
+}
+
 // Reconstruction: anchors + codes -> values (interpolation_reverse
 // :2177-2207); PROG adds the previous values (interpolation_progressive_reverse
 // :2209-2239, shmem2global_data_progressive :1123-1147).  All codes the tile
 // can use are fetched up front with kPrefetch loads in flight per thread.
 template <class T, bool PROG, int PART>
-__global__ void __launch_bounds__(kPredThreads, 5)
+__global__ void __launch_bounds__(kPredThreads, PART == 0 ? 5 : 3)
 reconstruct_kernel(const int32_t* __restrict__ qc, const T* __restrict__ anchors, Geometry g,
                    const PredParams<T>* __restrict__ pp, const T* old, T* out) {
   constexpr bool EDGE = PART == 1;

@@ -13,6 +13,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/prism_b200.h"
@@ -1050,3 +1051,6 @@ int prism_lossless_encode_static(const uint8_t* d_planes, uint32_t nx, uint32_t 
   *size_out = padded;
   return PRISM_OK;
 }
+
+#include "batch_api.cuh"
+#include "server_api.cuh"

@@ -156,24 +156,19 @@ __device__ __forceinline__ void copy_out(uint8_t* dst, const uint8_t* src, int n
   if (tid < n - done) dst[done + tid] = src[done + tid];
 }
 
-// Persistent encoder: one CTA (512 threads, 32 bytes each) per 16 KiB chunk,
-// four CTAs per SM.
-__global__ void __launch_bounds__(kZThreads, 4)
-zbpc_encode_kernel(const uint8_t* __restrict__ planes, Geometry g, uint8_t* __restrict__ stream,
-                   unsigned long long* __restrict__ status, unsigned long long* __restrict__ ticket,
-                   uint64_t* __restrict__ comp_size_bp, uint64_t* __restrict__ lossless_size,
-                   int* __restrict__ error_flag, long long spin_limit) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  EncodeShared& sh = *reinterpret_cast<EncodeShared*>(smem_raw);
+// Encode chunk `id` of one field (status is that field's slice, so the
+// look-back ends at the field's first chunk).  All 512 threads of the CTA
+// call this; it ends with a barrier.
+__device__ __forceinline__ void encode_chunk(EncodeShared& sh, const uint8_t* __restrict__ planes, const Geometry& g,
+                                             uint8_t* __restrict__ stream, unsigned long long* __restrict__ status,
+                                             const int64_t id, uint64_t* __restrict__ comp_size_bp,
+                                             uint64_t* __restrict__ lossless_size, int* __restrict__ error_flag,
+                                             long long spin_limit) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int64_t chunks = g.chunks;
   uint16_t* sizes = reinterpret_cast<uint16_t*>(stream + 8);
   uint8_t* data_out = stream + 8 + 2 * chunks;
-  while (true) {
-    if (tid == 0) sh.ticket = (long long)atomicAdd(ticket, 1ull);
-    __syncthreads();
-    const int64_t id = sh.ticket;
-    if (id >= chunks) break;
+  {
     const ChunkLoc loc = locate_chunk(g, id);
     const int osize = loc.osize;
     // ---- load 32 bytes per thread (base and osize are multiples of 8) ----
@@ -333,6 +328,24 @@ zbpc_encode_kernel(const uint8_t* __restrict__ planes, Geometry g, uint8_t* __re
     }
     copy_out(data_out + offs, raw ? sh.in : sh.out, csize);
     __syncthreads();
+  }
+}
+
+// Persistent encoder: one CTA (512 threads, 32 bytes each) per 16 KiB chunk,
+// four CTAs per SM, chunks handed out in order by a ticket counter.
+__global__ void __launch_bounds__(kZThreads, 4)
+zbpc_encode_kernel(const uint8_t* __restrict__ planes, Geometry g, uint8_t* __restrict__ stream,
+                   unsigned long long* __restrict__ status, unsigned long long* __restrict__ ticket,
+                   uint64_t* __restrict__ comp_size_bp, uint64_t* __restrict__ lossless_size,
+                   int* __restrict__ error_flag, long long spin_limit) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  EncodeShared& sh = *reinterpret_cast<EncodeShared*>(smem_raw);
+  while (true) {
+    if (threadIdx.x == 0) sh.ticket = (long long)atomicAdd(ticket, 1ull);
+    __syncthreads();
+    const int64_t id = sh.ticket;
+    if (id >= g.chunks) break;
+    encode_chunk(sh, planes, g, stream, status, id, comp_size_bp, lossless_size, error_flag, spin_limit);
   }
 }
 

@@ -100,3 +100,68 @@ GENERATORS = {"sinusoid": sinusoid, "grf": grf, "voronoi": voronoi}
 def make(kind, shape, dtype, seed):
     """Dispatch by generator name; ``shape`` is (nz, ny, nx)."""
     return GENERATORS[kind](tuple(shape), dtype=np.dtype(dtype), seed=seed)
+
+
+# ---- device-side generators (torch, for benchmark-scale inputs) -------------
+# Same families as above, generated on the GPU so that multi-GB inputs take
+# seconds; the values differ from the numpy versions (different RNG streams).
+
+def device_sinusoid(shape, dtype, seed, device="cuda", waves=8, noise=1e-3):
+    import torch
+    nz, ny, nx = shape
+    rng = np.random.default_rng(seed)
+    amp = rng.uniform(0.1, 1.0, waves)
+    phase = rng.uniform(0.0, 2 * np.pi, waves)
+    k = rng.integers(1, 9, size=(waves, 3))
+    z = torch.arange(nz, device=device, dtype=torch.float64)[:, None, None] / max(nz, 1)
+    y = torch.arange(ny, device=device, dtype=torch.float64)[None, :, None] / max(ny, 1)
+    x = torch.arange(nx, device=device, dtype=torch.float64)[None, None, :] / max(nx, 1)
+    out = torch.zeros(shape, device=device, dtype=torch.float64)
+    for i in range(waves):
+        out += float(amp[i]) * torch.sin(2 * np.pi * (int(k[i, 0]) * x + int(k[i, 1]) * y + int(k[i, 2]) * z)
+                                         + float(phase[i]))
+    g = torch.Generator(device=device)
+    g.manual_seed(int(seed))
+    out += noise * torch.randn(shape, device=device, dtype=torch.float64, generator=g)
+    return out.to(torch.float32 if np.dtype(dtype) == np.float32 else torch.float64)
+
+
+def device_grf(shape, dtype, seed, device="cuda", slope=-5.0 / 3.0, lo=0.9, hi=3.0):
+    import torch
+    nz, ny, nx = shape
+    kz = torch.fft.fftfreq(nz, device=device, dtype=torch.float32)[:, None, None]
+    ky = torch.fft.fftfreq(ny, device=device, dtype=torch.float32)[None, :, None]
+    kx = torch.fft.rfftfreq(nx, device=device, dtype=torch.float32)[None, None, :]
+    kk = torch.sqrt(kz * kz + ky * ky + kx * kx)
+    kk[0, 0, 0] = 1.0
+    amp = kk ** (slope / 2.0)
+    amp[0, 0, 0] = 0.0
+    g = torch.Generator(device=device)
+    g.manual_seed(int(seed))
+    spec = torch.complex(torch.randn(amp.shape, device=device, generator=g),
+                         torch.randn(amp.shape, device=device, generator=g)) * amp
+    del kk, amp
+    f = torch.fft.irfftn(spec, s=shape, dim=(0, 1, 2))
+    del spec
+    fmin, fmax = f.min(), f.max()
+    f = lo + (hi - lo) * (f - fmin) / (fmax - fmin)
+    return f.to(torch.float32 if np.dtype(dtype) == np.float32 else torch.float64)
+
+
+def uneven_mix(count=64, seed=47, lo=32, hi=2048, cap3=512 ** 3):
+    """The uneven batch: `count` fields, dimensionality uniform on {1, 2, 3},
+    per-axis extents log-uniform in [lo, hi], 3-D volumes capped at `cap3`
+    values (axes scaled down together), alternating smooth sinusoid sums and
+    k^-5/3 random fields.  Returns [(kind, (nx, ny, nz))].  The default seed
+    draws 5.96 GB of float32 in total (most draws give 3-4 GB; the batch is
+    specified at about 6 GB)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        d = int(rng.integers(1, 4))
+        ext = np.exp(rng.uniform(np.log(lo), np.log(hi), d))
+        if d == 3 and np.prod(ext) > cap3:
+            ext = ext * (cap3 / np.prod(ext)) ** (1.0 / 3.0)
+        e = [max(lo, int(v)) for v in ext] + [1] * (3 - d)
+        out.append(("sinusoid" if i % 2 == 0 else "grf", (e[0], e[1], e[2])))
+    return out
