@@ -126,6 +126,22 @@ def dist_setup():
     return world, rank, local
 
 
+def max_over_ranks(ms, world, device="cuda"):
+    """The slowest rank's time (all ranks take part; no-op for one rank)."""
+    if world <= 1:
+        return float(ms)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(ms)], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def weak_throughput(bytes_per_step_per_rank, steps, world, ms_max):
+    """Whole-job GB/s: every rank processed its own bytes in the slowest rank's time."""
+    return bytes_per_step_per_rank * steps * world / (ms_max / 1e3) / 1e9
+
+
 # ---------------------------------------------------------------- CPU arm
 def cpu_sample_run(data_slab, steps):
     """Oracle (C, OpenMP over tiles and chunks) on the slab; returns seconds
@@ -251,12 +267,9 @@ def run_prism(args, world, rank, local):
     stage = h.stage_times(reset=True)
     launches = h.launches() - launches0
     h.profile(False)
-    ms_t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
+    ms_max = max_over_ranks(ms, world)
     bytes_step = field_bytes * (1 + len(TARGETS))
-    value = bytes_step * args.steps * world / (ms_max / 1e3) / 1e9
+    value = weak_throughput(bytes_step, args.steps, world, ms_max)
 
     # ---- end-to-end through host buffers (C ABI, copies inside the region) ----
     h_in = torch.from_numpy(host).pin_memory()
@@ -291,10 +304,7 @@ def run_prism(args, world, rank, local):
         csz = e2e_workflow()
     e1.record(stream)
     barrier()
-    e2e_ms = torch.tensor([e0.elapsed_time(e1)], device="cuda", dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(e2e_ms, op=dist.ReduceOp.MAX)
-    e2e_value = bytes_step * args.steps * world / (float(e2e_ms.item()) / 1e3) / 1e9
+    e2e_value = weak_throughput(bytes_step, args.steps, world, max_over_ranks(e0.elapsed_time(e1), world))
 
     # ---- roofline of the dominant stage ----
     peak, peak_kind = measured_peak()
@@ -327,6 +337,13 @@ def run_prism(args, world, rank, local):
         dist.destroy_process_group()
     if rank != 0:
         return 0
+    # free the single-field buffers before the batch and serving parts
+    del d_in, d_cont, values, d_cont2, comp, h
+    torch.cuda.empty_cache()
+    batched = None if args.no_batch else run_batched(torch, P, args)
+    torch.cuda.empty_cache()
+    serving = None if args.no_serve else run_serving(torch, P, args)
+    torch.cuda.empty_cache()
     line = {
         "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -341,9 +358,139 @@ def run_prism(args, world, rank, local):
                 "d2h_bytes_per_step": csz + len(TARGETS) * field_bytes},
         "roofline": roofline, "stages": stages, "cpu_baseline": cpu, "gpu_launches": launches,
         "clocks": clk,
+        "batched": batched, "serving": serving,
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+# ---------------------------------------------------------------- batched
+def run_batched(torch, P, args):
+    """The uneven 64-field float32 batch at REL 1e-3: batched pipeline (one
+    launch per stage, CUDA graph) against per-field prism_compress calls on
+    the same device-resident fields; containers compared byte for byte."""
+    from prism_b200 import fields
+    mix = fields.uneven_mix()
+    items = []
+    for i, (kind, (nx, ny, nz)) in enumerate(mix):
+        gen = fields.device_sinusoid if kind == "sinusoid" else fields.device_grf
+        d = gen((nz, ny, nx), np.float32, 100 + i).contiguous()
+        items.append((P.Context(nx, ny, nz, np.dtype(np.float32), P.REL, 1e-3, False), d))
+    torch.cuda.synchronize()
+    total = sum(d.numel() * 4 for _, d in items)
+    t0 = time.time()
+    b = P.Batch(items, use_graph=True)
+    plan_s = time.time() - t0
+    reps = max(3, min(args.steps, 10))
+    for _ in range(args.warmup):
+        b.compress()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record()
+    for _ in range(reps):
+        conts, _ = b.compress()
+    ev1.record()
+    torch.cuda.synchronize()
+    batch_ms = ev0.elapsed_time(ev1) / reps
+    h = P.Handle()
+    comps = [P.Compressor(c, h) for c, _ in items]
+    outs = [torch.empty(c.max_container_size(), dtype=torch.uint8, device="cuda") for c in comps]
+    for _ in range(args.warmup):
+        for c, (_, d), o in zip(comps, items, outs):
+            c.compress_pipeline(d, o)
+    torch.cuda.synchronize()
+    ev0.record()
+    for _ in range(reps):
+        ref = [c.compress_pipeline(d, o) for c, (_, d), o in zip(comps, items, outs)]
+    ev1.record()
+    torch.cuda.synchronize()
+    plain_ms = ev0.elapsed_time(ev1) / reps
+    identical = all(torch.equal(a, r) for a, r in zip(conts, ref))
+    cbytes = sum(int(c.numel()) for c in conts)
+    sch = b.schedule()
+    b.close()
+    del items, outs, conts, ref
+    return {"workload": "64 uneven float32 fields (1-D/2-D/3-D, extents log-uniform 32..2048, 3-D capped at "
+                        "512^3 values, sinusoid sums and k^-5/3 fields alternating), REL 1e-3, compress",
+            "fields": len(mix), "input_bytes": total, "container_bytes": cbytes,
+            "batched_GBps": total / batch_ms / 1e6, "per_field_GBps": total / plain_ms / 1e6,
+            "batched_ms": batch_ms, "per_field_ms": plain_ms, "speedup": plain_ms / batch_ms,
+            "identical_containers": identical, "runs": reps, "plan_s": plan_s, "schedule": sch,
+            "data": "synthetic, generated on the device"}
+
+
+# ---------------------------------------------------------------- serving
+def run_serving(torch, P, args, nfields=32, rate=200.0, seconds=5.0, slots=4, pool=16):
+    """Progressive retrievals against device-resident -prog containers: Poisson
+    arrivals (rate per second), Zipf(1.1) field choice, REL bounds log-uniform
+    in [1e-6, 1e-1]; latency p50/p99 from arrival to completion."""
+    from prism_b200 import fields
+    rng = np.random.default_rng(11)
+    sizes = np.exp(rng.uniform(np.log(8e6), np.log(1e9), nfields))
+    ctxs, conts = [], []
+    h = P.Handle()
+    for i, sb in enumerate(sizes):
+        n = int(sb / 8)
+        nz = max(16, int(round((n / 2.25) ** (1 / 3))))
+        nx = ny = max(16, int(round((n / nz) ** 0.5)))
+        gen = fields.device_grf if i % 2 else fields.device_sinusoid
+        d = gen((nz, ny, nx), np.float64, 200 + i).contiguous()
+        ctx = P.Context(nx, ny, nz, np.dtype(np.float64), P.REL, 1e-6, True)
+        conts.append(P.Compressor(ctx, h).compress_pipeline(d).clone())
+        ctxs.append(ctx)
+        del d
+    torch.cuda.synchronize()
+    free, _ = torch.cuda.mem_get_info()
+    maxbytes = max(int(np.prod(c.shape)) * 8 for c in ctxs)
+    budget = int(min(150e9, free - (pool + 2) * maxbytes - (4 << 30)))
+    srv = P.Server(budget, slots=slots)
+    ids = [srv.add_field(c, k) for c, k in zip(ctxs, conts)]
+    del conts
+    torch.cuda.empty_cache()
+    nreq = int(rate * seconds)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, nreq))
+    ranks = np.arange(1, nfields + 1, dtype=np.float64)
+    pz = ranks ** -1.1
+    pz /= pz.sum()
+    pick = rng.choice(nfields, size=nreq, p=pz)
+    targets = np.exp(rng.uniform(np.log(1e-6), np.log(1e-1), nreq))
+    bufs = [torch.empty(maxbytes // 8, dtype=torch.float64, device="cuda") for _ in range(pool)]
+    free_bufs = list(range(pool))
+    inflight = []  # (request id, buffer, arrival time)
+    e2e = []
+    t_start = time.perf_counter()
+
+    def finish_one():
+        rid, bi, t_arr = inflight.pop(0)
+        srv.wait(rid)
+        e2e.append((time.perf_counter() - t_start - t_arr) * 1e3)
+        free_bufs.append(bi)
+
+    for k in range(nreq):
+        now = time.perf_counter() - t_start
+        if arrivals[k] > now:
+            time.sleep(arrivals[k] - now)
+        while not free_bufs:
+            finish_one()
+        bi = free_bufs.pop()
+        f = int(pick[k])
+        out = bufs[bi][: int(np.prod(ctxs[f].shape))].view(ctxs[f].shape)
+        inflight.append((srv.submit(ids[f], float(targets[k]), out), bi, float(arrivals[k])))
+    while inflight:
+        finish_one()
+    wall = time.perf_counter() - t_start
+    st = srv.stats()
+    srv.close()
+    e2e.sort()
+    q = lambda p: e2e[min(len(e2e) - 1, int(p * (len(e2e) - 1) + 0.5))]
+    return {"workload": f"{nfields} f64 -prog REL 1e-6 containers of 8 MB-1 GB fields, Poisson {rate:g}/s for "
+                        f"{seconds:g} s, Zipf(1.1) fields, REL targets log-uniform [1e-6, 1e-1]",
+            "requests": nreq, "slots": slots, "hbm_budget_bytes": budget,
+            "p50_ms": q(0.50), "p99_ms": q(0.99), "server_p50_ms": st["p50_ms"], "server_p99_ms": st["p99_ms"],
+            "requests_per_s": nreq / wall, "delivered_GBps": st["bytes_out"] / wall / 1e9,
+            "cache_hits": st["cache_hits"], "shared": st["shared"], "evictions": st["evictions"],
+            "failed": st["failed"], "peak_resident_bytes": st["bytes_peak"],
+            "data": "synthetic, generated on the device; scaled from 256 fields / 60 s to keep the run short"}
 
 
 def main():
@@ -353,6 +500,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="prism", choices=["prism", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-compression measurement")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving measurement")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":

@@ -211,8 +211,9 @@ int prism_batch_create(const prism_field_desc* fields, int n, int use_graph, pri
  * buffers; sizes_out[i] receives field i's container size and flags_out
  * (may be NULL) its use_md[4], reverse[4].  Waits for `stream`. */
 int prism_batch_compress(prism_batch* b, void* stream, uint64_t* sizes_out, uint8_t* flags_out);
-/* The tuned schedule: predictor CTAs per SM for float and double fields,
- * encoder CTAs per SM, the tuned stage times (ms) and kernels per run. */
+/* The tuned schedule: predictor CTAs per SM for float and double fields (0 =
+ * one CTA per tile instead of persistent CTAs), encoder CTAs per SM, the
+ * tuned stage times (ms) and kernels per run. */
 int prism_batch_schedule(const prism_batch* b, int pred_ctas_per_sm[2], int* enc_ctas_per_sm, double tuned_ms[2],
                          uint64_t* launches_per_run);
 const char* prism_batch_last_error(const prism_batch* b);

@@ -99,7 +99,18 @@ batch_extrema_kernel(const BatchField* __restrict__ fields, const int* __restric
     const uint64_t s0 = (item - prefix[e]) * kBatchExtSeg;
     const uint64_t s1 = min(s0 + kBatchExtSeg, f.g.n);
     T mn = in[s0], mx = in[s0];
-    for (uint64_t i = s0 + threadIdx.x; i < s1; i += blockDim.x) {
+    uint64_t i = s0 + threadIdx.x;
+    for (; i + 3 * blockDim.x < s1; i += 4 * blockDim.x) {  // four loads in flight
+      T v[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) v[k] = __ldg(in + i + k * blockDim.x);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        mn = v[k] < mn ? v[k] : mn;
+        mx = v[k] > mx ? v[k] : mx;
+      }
+    }
+    for (; i < s1; i += blockDim.x) {
       T v = __ldg(in + i);
       mn = v < mn ? v : mn;
       mx = v > mx ? v : mx;
@@ -181,15 +192,53 @@ __global__ void batch_zero_kernel(const BatchZero* __restrict__ segs, int nseg) 
   }
 }
 
-// Persistent predictor over the tiles of part PART (0 interior, 1 edge) of
-// every group field; CTAs take tiles from `counter`.
+// One tile of a batch field: geometry copied to shared memory (the
+// per-field kernel has it in its parameters) and read from there at each use.
+template <class T, int PART>
+__device__ __forceinline__ void batch_tile(CompressSmem<T>& sm, Geometry& sg, const BatchField* f, uint32_t local) {
+  {
+    const uint32_t* src = reinterpret_cast<const uint32_t*>(&f->g);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(&sg);
+    for (int i = threadIdx.x; i < (int)(sizeof(Geometry) / 4); i += kPredThreads) dst[i] = src[i];
+  }
+  __syncthreads();
+  const volatile Geometry& gv = sg;
+  uint32_t bi[3];
+  tile_of_index<PART, volatile Geometry>(gv, local, bi);
+  compress_tile<T, PART == 1, volatile Geometry>(sm, reinterpret_cast<const T*>(f->in), gv, bi,
+                                                 reinterpret_cast<const PredParams<T>*>(f->st->params),
+                                                 reinterpret_cast<T*>(f->anchors), f->qc);
+}
+
+// the same, out of line: keeps the persistent loop's registers separate
+template <class T, int PART>
+__device__ __noinline__ void batch_tile_call(CompressSmem<T>& sm, Geometry& sg, const BatchField* f, uint32_t local) {
+  batch_tile<T, PART>(sm, sg, f, local);
+}
+
+// Predictor over the tiles of part PART (0 interior, 1 edge) of every group
+// field, one CTA per tile.
 template <class T, int PART>
 __global__ void __launch_bounds__(kPredThreads, 3)
 batch_predict_kernel(const BatchField* __restrict__ fields, const int* __restrict__ gidx,
-                     const uint64_t* __restrict__ prefix, int n, uint64_t items,
-                     unsigned long long* __restrict__ counter) {
+                     const uint64_t* __restrict__ prefix, int n, uint64_t items) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  CompressSmem<T>& sm = *reinterpret_cast<CompressSmem<T>*>(smem_raw);
+  __shared__ __align__(16) Geometry sg;
+  const uint64_t item = blockIdx.x;
+  if (item >= items) return;
+  const int e = find_field(prefix, n, item);
+  batch_tile<T, PART>(*reinterpret_cast<CompressSmem<T>*>(smem_raw), sg, &fields[gidx[e]],
+                      (uint32_t)(item - prefix[e]));
+}
+
+// The same with persistent CTAs taking tiles from a device counter.
+template <class T, int PART>
+__global__ void __launch_bounds__(kPredThreads, 3)
+batch_predict_persistent_kernel(const BatchField* __restrict__ fields, const int* __restrict__ gidx,
+                                const uint64_t* __restrict__ prefix, int n, uint64_t items,
+                                unsigned long long* __restrict__ counter) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ __align__(16) Geometry sg;
   __shared__ unsigned long long next;
   while (true) {
     __syncthreads();  // the previous tile no longer reads shared memory
@@ -198,12 +247,8 @@ batch_predict_kernel(const BatchField* __restrict__ fields, const int* __restric
     const uint64_t item = next;
     if (item >= items) break;
     const int e = find_field(prefix, n, item);
-    const BatchField& f = fields[gidx[e]];
-    uint32_t bi[3];
-    tile_of_index<PART>(f.g, (uint32_t)(item - prefix[e]), bi);
-    compress_tile<T, PART == 1>(sm, reinterpret_cast<const T*>(f.in), f.g, bi,
-                                reinterpret_cast<const PredParams<T>*>(f.st->params),
-                                reinterpret_cast<T*>(f.anchors), f.qc);
+    batch_tile_call<T, PART>(*reinterpret_cast<CompressSmem<T>*>(smem_raw), sg, &fields[gidx[e]],
+                             (uint32_t)(item - prefix[e]));
   }
 }
 

@@ -116,15 +116,24 @@ template <class T>
 int enqueue_group_predict(prism_batch* b, const prism_batch::Group& gr, int g, int ctas, cudaStream_t st,
                           uint64_t& launches) {
   const int smem = compress_smem_bytes<T>();
+  // ctas > 0: persistent CTAs (ctas per SM) on the tile counter; 0: one CTA
+  // per tile
   for (int part = 0; part < 2; ++part) {
     if (!gr.tiles[part]) continue;
-    unsigned grid = (unsigned)std::min<uint64_t>(gr.tiles[part], (uint64_t)b->sm_count * ctas);
-    if (part == 0)
-      batch_predict_kernel<T, 0><<<grid, kPredThreads, smem, st>>>(b->d_fields, gr.d_idx, gr.d_tile_prefix[0], gr.n,
-                                                                   gr.tiles[0], b->d_counters + 2 * g);
+    unsigned grid = ctas > 0 ? (unsigned)std::min<uint64_t>(gr.tiles[part], (uint64_t)b->sm_count * ctas)
+                             : (unsigned)gr.tiles[part];
+    unsigned long long* counter = b->d_counters + 2 * g + part;
+    const uint64_t* pre = gr.d_tile_prefix[part];
+    if (ctas == 0 && part == 0)
+      batch_predict_kernel<T, 0><<<grid, kPredThreads, smem, st>>>(b->d_fields, gr.d_idx, pre, gr.n, gr.tiles[0]);
+    else if (ctas == 0)
+      batch_predict_kernel<T, 1><<<grid, kPredThreads, smem, st>>>(b->d_fields, gr.d_idx, pre, gr.n, gr.tiles[1]);
+    else if (part == 0)
+      batch_predict_persistent_kernel<T, 0><<<grid, kPredThreads, smem, st>>>(b->d_fields, gr.d_idx, pre, gr.n,
+                                                                              gr.tiles[0], counter);
     else
-      batch_predict_kernel<T, 1><<<grid, kPredThreads, smem, st>>>(b->d_fields, gr.d_idx, gr.d_tile_prefix[1], gr.n,
-                                                                   gr.tiles[1], b->d_counters + 2 * g + 1);
+      batch_predict_persistent_kernel<T, 1><<<grid, kPredThreads, smem, st>>>(b->d_fields, gr.d_idx, pre, gr.n,
+                                                                              gr.tiles[1], counter);
     ++launches;
   }
   BCK(cudaGetLastError());
@@ -217,8 +226,9 @@ int time_stage(prism_batch* b, cudaStream_t st, Fn fn, double* ms) {
   return rc;
 }
 
-// Schedule tuner: CTAs per SM of the persistent predictor (per dtype) and of
-// the persistent encoder, chosen by timing every feasible value on the batch.
+// Schedule tuner: for the predictor (per dtype) one CTA per tile or
+// persistent CTAs with 1..max per SM, for the encoder 1..max persistent CTAs
+// per SM; every feasible value is timed on the batch and the fastest kept.
 int tune_schedule(prism_batch* b, cudaStream_t st) {
   uint64_t launches = 0;
   int rc = enqueue_all(b, st, launches);  // warm-up; leaves params and planes in place
@@ -228,7 +238,7 @@ int tune_schedule(prism_batch* b, cudaStream_t st) {
     if (!b->grp[g].n) continue;
     double best = 1e30;
     int pick = b->pred_max[g];
-    for (int c = 1; c <= b->pred_max[g]; ++c) {
+    for (int c = 0; c <= b->pred_max[g]; ++c) {  // 0: one CTA per tile
       double ms = 0;
       rc = time_stage(b, st, [&]() -> int {
         cudaMemsetAsync(b->d_counters + 2 * g, 0, 2 * sizeof(unsigned long long), st);
@@ -433,14 +443,27 @@ int batch_plan(prism_batch* b) {
   }
   // ---- occupancy limits of the persistent kernels ----
   int rc;
-  if ((rc = max_ctas<batch_predict_kernel<float, 0>>(b, kPredThreads, compress_smem_bytes<float>(), &b->pred_max[0])))
+  int dummy = 0;
+  if ((rc = max_ctas<batch_predict_kernel<float, 0>>(b, kPredThreads, compress_smem_bytes<float>(), &dummy))) return rc;
+  if ((rc = max_ctas<batch_predict_kernel<float, 1>>(b, kPredThreads, compress_smem_bytes<float>(), &dummy))) return rc;
+  if ((rc = max_ctas<batch_predict_kernel<double, 0>>(b, kPredThreads, compress_smem_bytes<double>(), &dummy)))
     return rc;
-  if ((rc = max_ctas<batch_predict_kernel<float, 1>>(b, kPredThreads, compress_smem_bytes<float>(), &b->pred_max[0])))
+  if ((rc = max_ctas<batch_predict_kernel<double, 1>>(b, kPredThreads, compress_smem_bytes<double>(), &dummy)))
     return rc;
-  if ((rc = max_ctas<batch_predict_kernel<double, 0>>(b, kPredThreads, compress_smem_bytes<double>(), &b->pred_max[1])))
+  if ((rc = max_ctas<batch_predict_persistent_kernel<float, 0>>(b, kPredThreads, compress_smem_bytes<float>(),
+                                                                &b->pred_max[0])))
     return rc;
-  if ((rc = max_ctas<batch_predict_kernel<double, 1>>(b, kPredThreads, compress_smem_bytes<double>(), &b->pred_max[1])))
+  if ((rc = max_ctas<batch_predict_persistent_kernel<float, 1>>(b, kPredThreads, compress_smem_bytes<float>(),
+                                                                &dummy)))
     return rc;
+  b->pred_max[0] = std::min(b->pred_max[0], dummy);
+  if ((rc = max_ctas<batch_predict_persistent_kernel<double, 0>>(b, kPredThreads, compress_smem_bytes<double>(),
+                                                                 &b->pred_max[1])))
+    return rc;
+  if ((rc = max_ctas<batch_predict_persistent_kernel<double, 1>>(b, kPredThreads, compress_smem_bytes<double>(),
+                                                                 &dummy)))
+    return rc;
+  b->pred_max[1] = std::min(b->pred_max[1], dummy);
   if ((rc = max_ctas<batch_encode_kernel>(b, kZThreads, (int)sizeof(EncodeShared), &b->enc_max))) return rc;
   b->pred_ctas[0] = b->pred_max[0];
   b->pred_ctas[1] = b->pred_max[1];

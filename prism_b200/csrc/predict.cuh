@@ -492,8 +492,8 @@ PRISM_HD uint64_t tiles_in_part(const Geometry& g, int part) {
   return part == 0 ? inner : (uint64_t)g.ax * g.ay * g.az - inner;
 }
 
-template <int PART>
-__device__ __forceinline__ void tile_of_index(const Geometry& g, uint32_t j, uint32_t bi[3]) {
+template <int PART, class G = Geometry>
+__device__ __forceinline__ void tile_of_index(const G& g, uint32_t j, uint32_t bi[3]) {
   if (PART == 0) {
     bi[0] = j % (g.ax - 1); bi[1] = (j / (g.ax - 1)) % (g.ay - 1); bi[2] = j / ((g.ax - 1) * (g.ay - 1));
     return;
@@ -519,7 +519,8 @@ struct TileFrame {
   AxisLimits lim;
 };
 
-__device__ __forceinline__ void tile_frame(const Geometry& g, const uint32_t bi[3], TileFrame& f) {
+template <class G>
+__device__ __forceinline__ void tile_frame(const G& g, const uint32_t bi[3], TileFrame& f) {
   const uint32_t gd[3] = {g.ax, g.ay, g.az}, dim[3] = {g.nx, g.ny, g.nz};
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
@@ -542,7 +543,8 @@ __device__ __forceinline__ int win_level(int x, int y, int z) { return __ffs(x |
 
 // Level-major slot of a point whose level (0..3) is known (the formula of
 // level_major_index without its level search).
-__device__ __forceinline__ uint64_t lm_slot(const Geometry& g, int level, uint64_t gx, uint64_t gy, uint64_t gz) {
+template <class G>
+__device__ __forceinline__ uint64_t lm_slot(const G& g, int level, uint64_t gx, uint64_t gy, uint64_t gz) {
   gx >>= level; gy >>= level; gz >>= level;
   uint64_t gid = gx + gy * g.leaps[level][0] + gz * g.leaps[level][1];
   gid += g.lm_prefix[level] - ((gz + 1) >> 1) * g.leaps[level + 1][1] -
@@ -554,7 +556,8 @@ __device__ __forceinline__ uint64_t lm_slot(const Geometry& g, int level, uint64
 // Row table: rows[(z*17 + y)] = level-0 slot of window point (0, y, z) minus
 // the x-dependent part, so that a level-0 point's slot is
 // rows[row] + x - (y, z both even ? (x + 1) / 2 : 0) (x, gs[0] even).
-__device__ __forceinline__ void fill_rows(const Geometry& g, const TileFrame& f, uint64_t* rows) {
+template <class G>
+__device__ __forceinline__ void fill_rows(const G& g, const TileFrame& f, uint64_t* rows) {
   for (int r = threadIdx.x; r < kWin * kWin; r += kPredThreads) {
     const uint64_t gy = f.gs[1] + r % kWin, gz = f.gs[2] + r / kWin;
     uint64_t base = (uint64_t)f.gs[0] + gy * g.leaps[0][0] + gz * g.leaps[0][1] + g.lm_prefix[0] -
@@ -564,7 +567,8 @@ __device__ __forceinline__ void fill_rows(const Geometry& g, const TileFrame& f,
   }
 }
 
-__device__ __forceinline__ uint64_t slot_of(const Geometry& g, const TileFrame& f, const uint64_t* rows, int lv,
+template <class G>
+__device__ __forceinline__ uint64_t slot_of(const G& g, const TileFrame& f, const uint64_t* rows, int lv,
                                             int x, int y, int z) {
   if (lv == 0) {
     const int row = z * kWin + y;
@@ -599,8 +603,8 @@ struct ReconSmem {
 // One tile of the compression (the body of predict_compress_kernel and of the
 // batched persistent kernel).  The caller guarantees that no thread still
 // reads `sm` from a previous tile.
-template <class T, bool EDGE>
-__device__ __forceinline__ void compress_tile(CompressSmem<T>& sm, const T* __restrict__ data, const Geometry& g,
+template <class T, bool EDGE, class G = Geometry>
+__device__ __forceinline__ void compress_tile(CompressSmem<T>& sm, const T* __restrict__ data, const G& g,
                                               const uint32_t bi[3], const PredParams<T>* __restrict__ pp,
                                               T* __restrict__ anchors, int32_t* __restrict__ qc) {
   TileFrame f;

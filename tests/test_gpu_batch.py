@@ -55,7 +55,9 @@ def test_batch_matches_per_field_containers(env, use_graph):
             assert np.array_equal(got, ref), (i, MIX[i], rep)
             assert fl == ref_flags, (i, fl, ref_flags)
     sch = b.schedule()
-    assert sch["predict_ctas_per_sm"][0] >= 1 and sch["encode_ctas_per_sm"] >= 1
+    # 0 = one CTA per tile, else persistent CTAs per SM
+    assert sch["predict_ctas_per_sm"][0] >= 0 and sch["encode_ctas_per_sm"] >= 1
+    assert sch["launches_per_run"] > 0
     b.close()
 
 
