@@ -183,6 +183,33 @@ int prism_lossless_encode_static(const uint8_t* d_planes, uint32_t nx, uint32_t 
 int prism_find_strategy(prism_handle* h, const uint64_t comp_size_bp[128], double eb,
                         double target_error, int begin[4], int end[4], int* maxlevel, void* stream);
 
+/* Error statistics of a reconstruction against the original (both device
+ * arrays of n values): out = {max |error|, max |error| / range, PSNR, NRMSE,
+ * min, max (of the original), sum of squared errors}; *max_err_index = first
+ * index with the max error.  Replaces statistic (include/utils/analyze.hpp:
+ * 5-73), which loops over host copies. */
+int prism_statistics(prism_handle* h, const void* d_original, const void* d_data, int dtype_size, uint64_t n,
+                     double out[7], uint64_t* max_err_index, void* stream);
+
+/* ---- container files ----------------------------------------------------
+ * Save a device-resident container to `path`: device-to-host copies through
+ * two pinned staging buffers overlap the file writes.  Waits for `stream`. */
+int prism_file_save(const char* path, const void* d_container, uint64_t size, void* stream);
+
+typedef struct prism_file prism_file;
+/* Open a -prog container file for progressive retrieval.  Reads only the
+ * stream header, the chunk size table and the trailer; later steps read only
+ * the chunks of the planes they add.  Replaces the reference's whole-file
+ * reload per target (src/prism.cu:131-135). */
+int prism_file_open(prism_handle* h, const char* path, int dtype_size, uint32_t nx, uint32_t ny, uint32_t nz,
+                    int mode, double bound, prism_file** out);
+/* One progressive step from the file: values equal prism_progressive_step on
+ * the whole container. */
+int prism_file_step(prism_file* f, double target_error, void* d_values, void* stream);
+/* File size, bytes read from it so far, planes loaded per level. */
+int prism_file_info(const prism_file* f, uint64_t* file_bytes, uint64_t* bytes_read, int end[4]);
+void prism_file_close(prism_file* f);
+
 /* ---- batched compression ----------------------------------------------
  * Many fields of uneven shapes compressed by one launch per pipeline stage;
  * no counterpart in the reference, whose pipeline handles one field per call
@@ -232,7 +259,9 @@ typedef struct prism_server prism_server;
 typedef struct prism_server_stats {
   uint64_t completed, cache_hits, shared, evictions, failed;
   uint64_t bytes_out, bytes_resident, bytes_reserved, bytes_peak;
-  double p50_ms, p99_ms, mean_ms, max_ms, elapsed_s;
+  double p50_ms, p99_ms, mean_ms, max_ms, elapsed_s;  /* submit -> completion */
+  double queue_p50_ms, queue_p99_ms;                  /* submit -> a slot takes it */
+  double service_p50_ms, service_p99_ms;              /* slot start -> completion */
 } prism_server_stats;
 
 /* hbm_budget: bytes of device memory the server may hold (containers,
@@ -252,6 +281,8 @@ int prism_server_submit(prism_server* s, int field_id, double target_error, void
  * Returns the request's status. */
 int prism_server_wait(prism_server* s, uint64_t request_id, double* latency_ms, int end[4], int* maxlevel,
                       int* from_cache);
+/* Non-blocking: *done = 1 once the request has completed (then wait). */
+int prism_server_poll(prism_server* s, uint64_t request_id, int* done);
 /* Latency percentiles and counters of the completed requests. */
 int prism_server_stats_get(prism_server* s, prism_server_stats* out, int reset);
 void prism_server_destroy(prism_server* s);

@@ -80,11 +80,18 @@ def lib():
         l.prism_batch_last_error.argtypes = [vp]
         l.prism_batch_last_error.restype = C.c_char_p
         l.prism_batch_destroy.argtypes = [vp]
+        l.prism_statistics.argtypes = [vp, vp, vp, i32, u64, vp, C.POINTER(u64), vp]
+        l.prism_file_save.argtypes = [C.c_char_p, vp, u64, vp]
+        l.prism_file_open.argtypes = [vp, C.c_char_p, i32, u32, u32, u32, i32, dbl, C.POINTER(vp)]
+        l.prism_file_step.argtypes = [vp, dbl, vp, vp]
+        l.prism_file_info.argtypes = [vp, C.POINTER(u64), C.POINTER(u64), vp]
+        l.prism_file_close.argtypes = [vp]
         l.prism_server_create.argtypes = [u64, i32, C.POINTER(vp)]
         l.prism_server_add_field.argtypes = [vp, vp, u64, i32, i32, u32, u32, u32, i32, dbl, C.POINTER(i32)]
         l.prism_server_submit.argtypes = [vp, i32, dbl, vp, i32, C.POINTER(u64)]
         l.prism_server_wait.argtypes = [vp, u64, C.POINTER(dbl), vp, C.POINTER(i32), C.POINTER(i32)]
         l.prism_server_stats_get.argtypes = [vp, vp, i32]
+        l.prism_server_poll.argtypes = [vp, u64, C.POINTER(i32)]
         l.prism_server_destroy.argtypes = [vp]
         l.prism_profile.argtypes = [vp, i32]
         l.prism_stage_times.argtypes = [vp, vp, vp, i32, i32]
@@ -104,7 +111,8 @@ EXPORTED = [
     "prism_profile", "prism_stage_times", "prism_launch_count", "prism_lossless_encode_static",
     "prism_batch_create", "prism_batch_compress", "prism_batch_schedule", "prism_batch_last_error",
     "prism_batch_destroy", "prism_server_create", "prism_server_add_field", "prism_server_submit",
-    "prism_server_wait", "prism_server_stats_get", "prism_server_destroy",
+    "prism_server_wait", "prism_server_stats_get", "prism_server_destroy", "prism_statistics", "prism_server_poll",
+    "prism_file_save", "prism_file_open", "prism_file_step", "prism_file_info", "prism_file_close",
 ]
 
 STAGES = ["extrema", "autotune", "predict", "shuffle", "encode", "trailer", "strategy", "decode",
@@ -140,6 +148,19 @@ class Handle:
         cnt = (C.c_int * 16)()
         n = lib().prism_stage_times(self.ptr, ms, cnt, 16, int(reset))
         return {STAGES[i]: (ms[i], cnt[i]) for i in range(min(n, len(STAGES)))}
+
+    def statistics(self, d_original, d_data):
+        """Error statistics of d_data against d_original (CUDA tensors)."""
+        torch = _torch()
+        out = (C.c_double * 7)()
+        idx = C.c_uint64()
+        self.check(lib().prism_statistics(self.ptr, C.c_void_p(d_original.data_ptr()), C.c_void_p(d_data.data_ptr()),
+                                          d_original.element_size(), d_original.numel(), out, C.byref(idx),
+                                          _stream(torch)), "prism_statistics")
+        keys = ["max_err", "max_rel_err", "psnr", "nrmse", "min", "max", "l2"]
+        r = dict(zip(keys, list(out)))
+        r["max_err_index"] = idx.value
+        return r
 
     def launches(self):
         return int(lib().prism_launch_count(self.ptr))
@@ -264,6 +285,51 @@ class Progressive:
             pass
 
 
+def save_container(path, d_cont):
+    """Write a device container (uint8 CUDA tensor) to a file."""
+    torch = _torch()
+    rc = lib().prism_file_save(str(path).encode(), C.c_void_p(d_cont.data_ptr()), d_cont.numel(), _stream(torch))
+    if rc:
+        raise PrismError(f"prism_file_save: {_STATUS.get(rc, rc)}")
+
+
+class FileProgressive:
+    """Progressive retrieval straight from a container file: each step reads
+    only the chunks of the planes it adds."""
+
+    def __init__(self, comp: Compressor, path):
+        torch = _torch()
+        c = comp.ctx
+        self.comp = comp
+        self.ptr = C.c_void_p()
+        comp.h.check(lib().prism_file_open(comp.h.ptr, str(path).encode(), c.tsize, c.nx, c.ny, c.nz, c.error_mode,
+                                           c.bound, C.byref(self.ptr)), "prism_file_open")
+        self.values = torch.zeros(c.shape, dtype=_torch_dtype(torch, c.dtype), device="cuda")
+
+    def step(self, target):
+        torch = _torch()
+        self.comp.h.check(lib().prism_file_step(self.ptr, target, C.c_void_p(self.values.data_ptr()), _stream(torch)),
+                          "prism_file_step")
+        return self.values
+
+    def info(self):
+        fb, br = C.c_uint64(), C.c_uint64()
+        end = (C.c_int * 4)()
+        lib().prism_file_info(self.ptr, C.byref(fb), C.byref(br), end)
+        return {"file_bytes": fb.value, "bytes_read": br.value, "end": list(end)}
+
+    def close(self):
+        if self.ptr:
+            lib().prism_file_close(self.ptr)
+            self.ptr = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class FieldDesc(C.Structure):
     """prism_field_desc: one field of a batch (device buffers)."""
     _fields_ = [("d_in", C.c_void_p), ("d_out", C.c_void_p), ("out_capacity", C.c_uint64), ("nx", C.c_uint32),
@@ -331,7 +397,8 @@ class Batch:
 class ServerStats(C.Structure):
     _fields_ = [(k, C.c_uint64) for k in ("completed", "cache_hits", "shared", "evictions", "failed", "bytes_out",
                                           "bytes_resident", "bytes_reserved", "bytes_peak")] + \
-               [(k, C.c_double) for k in ("p50_ms", "p99_ms", "mean_ms", "max_ms", "elapsed_s")]
+               [(k, C.c_double) for k in ("p50_ms", "p99_ms", "mean_ms", "max_ms", "elapsed_s", "queue_p50_ms",
+                                          "queue_p99_ms", "service_p50_ms", "service_p99_ms")]
 
 
 class Server:
@@ -379,6 +446,13 @@ class Server:
         if rc:
             raise PrismError(f"prism_server_wait: {_STATUS.get(rc, rc)}")
         return {"latency_ms": lat.value, "end": list(end), "maxlevel": ml.value, "from_cache": bool(hit.value)}
+
+    def done(self, request_id):
+        d = C.c_int()
+        rc = lib().prism_server_poll(self.ptr, C.c_uint64(request_id), C.byref(d))
+        if rc:
+            raise PrismError(f"prism_server_poll: {_STATUS.get(rc, rc)}")
+        return bool(d.value)
 
     def stats(self, reset=False):
         st = ServerStats()

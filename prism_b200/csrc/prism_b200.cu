@@ -21,6 +21,7 @@
 #include "bitplane.cuh"
 #include "geometry.h"
 #include "predict.cuh"
+#include "report.cuh"
 #include "strategy.cuh"
 #include "zbpc.cuh"
 
@@ -90,7 +91,37 @@ struct prism_handle {
   bool pending[kStCount] = {};
   double acc_ms[kStCount] = {};
   int acc_n[kStCount] = {};
+  // side stream for the edge-tile launches, which run beside the interior
+  // launch (the two write disjoint tiles)
+  cudaStream_t side = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
 };
+
+// Run `interior` on st and `edge` on the handle's side stream concurrently;
+// st waits for both before its next work.
+template <class FI, class FE>
+static cudaError_t fork_join(prism_handle* h, cudaStream_t st, bool have_interior, bool have_edge, FI interior,
+                             FE edge) {
+  if (!have_interior || !have_edge) {
+    if (have_interior) interior(st);
+    if (have_edge) edge(st);
+    return cudaGetLastError();
+  }
+  cudaError_t e = cudaSuccess;
+  if (!h->side) {
+    e = cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming);
+    if (e != cudaSuccess) return e;
+  }
+  if ((e = cudaEventRecord(h->fork, st)) != cudaSuccess) return e;
+  if ((e = cudaStreamWaitEvent(h->side, h->fork, 0)) != cudaSuccess) return e;
+  edge(h->side);
+  if ((e = cudaEventRecord(h->join, h->side)) != cudaSuccess) return e;
+  interior(st);
+  if ((e = cudaStreamWaitEvent(st, h->join, 0)) != cudaSuccess) return e;
+  return cudaGetLastError();
+}
 
 static void prof_begin(prism_handle* h, int stage, cudaStream_t st) {
   if (h->prof) cudaEventRecord(h->ev[stage][0], st);
@@ -191,9 +222,10 @@ static int launch_predict(prism_handle* h, const T* in, const Geometry& g, const
   CK(smem_limit<k0>(smem));
   CK(smem_limit<k1>(smem));
   uint64_t n0 = tiles_in_part(g, 0), n1 = tiles_in_part(g, 1);
-  if (n0) { k0<<<(unsigned)n0, kPredThreads, smem, st>>>(in, g, pp, anchors, qc); h->launches += 1; }
-  if (n1) { k1<<<(unsigned)n1, kPredThreads, smem, st>>>(in, g, pp, anchors, qc); h->launches += 1; }
-  CK(cudaGetLastError());
+  CK(fork_join(
+      h, st, n0 > 0, n1 > 0, [&](cudaStream_t s) { k0<<<(unsigned)n0, kPredThreads, smem, s>>>(in, g, pp, anchors, qc); },
+      [&](cudaStream_t s) { k1<<<(unsigned)n1, kPredThreads, smem, s>>>(in, g, pp, anchors, qc); }));
+  h->launches += (n0 > 0) + (n1 > 0);
   return PRISM_OK;
 }
 
@@ -206,9 +238,11 @@ static int launch_reconstruct(prism_handle* h, const int32_t* qc, const T* ancho
   CK(smem_limit<k0>(smem0));
   CK(smem_limit<k1>(smem1));
   uint64_t n0 = tiles_in_part(g, 0), n1 = tiles_in_part(g, 1);
-  if (n0) { k0<<<(unsigned)n0, kPredThreads, smem0, st>>>(qc, anchors, g, pp, old, out); h->launches += 1; }
-  if (n1) { k1<<<(unsigned)n1, kPredThreads, smem1, st>>>(qc, anchors, g, pp, old, out); h->launches += 1; }
-  CK(cudaGetLastError());
+  CK(fork_join(
+      h, st, n0 > 0, n1 > 0,
+      [&](cudaStream_t s) { k0<<<(unsigned)n0, kPredThreads, smem0, s>>>(qc, anchors, g, pp, old, out); },
+      [&](cudaStream_t s) { k1<<<(unsigned)n1, kPredThreads, smem1, s>>>(qc, anchors, g, pp, old, out); }));
+  h->launches += (n0 > 0) + (n1 > 0);
   return PRISM_OK;
 }
 
@@ -532,6 +566,9 @@ void prism_destroy(prism_handle* h) {
   for (int i = 0; i < kStCount; ++i)
     for (int j = 0; j < 2; ++j)
       if (h->ev[i][j]) cudaEventDestroy(h->ev[i][j]);
+  if (h->side) cudaStreamDestroy(h->side);
+  if (h->fork) cudaEventDestroy(h->fork);
+  if (h->join) cudaEventDestroy(h->join);
   if (h->host) cudaFreeHost(h->host);
   delete h;
 }
@@ -740,7 +777,21 @@ int prism_progressive_state(const prism_prog* p, int begin[4], int end[4], int* 
     if (end) end[i] = p->state.end[i];
   }
   if (maxlevel) *maxlevel = p->state.maxlevel;
-  if (loaded) *loaded = 0;
+  if (loaded) {
+    // payload bytes of every plane loaded so far: steps load [previous end,
+    // end), so the total is planes [0, end) (calculate_accumulate_size,
+    // analyze.hpp:118-159, summed over the steps)
+    uint64_t cum[128];
+    const uint8_t* tr = p->cont + (p->size - p->g.header_size);
+    if (cudaMemcpy(cum, tr + 16, sizeof(cum), cudaMemcpyDeviceToHost) != cudaSuccess) return PRISM_ERR_CUDA;
+    uint64_t total = 0;
+    for (int i = 0; i < 4; ++i)
+      for (int j = 0; j < p->state.end[i] && j < 32; ++j) {
+        const int k = i * 32 + j;
+        total += cum[k] - (k > 0 ? cum[k - 1] : 0);
+      }
+    *loaded = total;
+  }
   return PRISM_OK;
 }
 
@@ -1054,3 +1105,34 @@ int prism_lossless_encode_static(const uint8_t* d_planes, uint32_t nx, uint32_t 
 
 #include "batch_api.cuh"
 #include "server_api.cuh"
+#include "file_api.cuh"
+
+// ---- reconstruction error statistics (--report cr) ----
+int prism_statistics(prism_handle* h, const void* d_original, const void* d_data, int dtype_size, uint64_t n,
+                     double out[7], uint64_t* max_err_index, void* stream) {
+  if (!h || !d_original || !d_data || !out || n == 0 || (dtype_size != 4 && dtype_size != 8)) return PRISM_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int blocks = (int)std::min<uint64_t>((n + kStatThreads - 1) / kStatThreads, (uint64_t)h->sm_count * 8);
+  CKA(h->part.ensure(sizeof(StatPart) * blocks + 64));
+  StatPart* part = h->part.as<StatPart>();
+  if (dtype_size == 4)
+    stats_kernel<float><<<blocks, kStatThreads, 0, st>>>((const float*)d_original, (const float*)d_data, n, part);
+  else
+    stats_kernel<double><<<blocks, kStatThreads, 0, st>>>((const double*)d_original, (const double*)d_data, n, part);
+  stats_final_kernel<<<1, 32, 0, st>>>(part, blocks);
+  h->launches += 2;
+  CK(cudaGetLastError());
+  StatPart r;
+  CK(cudaMemcpyAsync(&r, part, sizeof(r), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  const double range = r.mx - r.mn, mse = r.l2 / (double)n;
+  out[0] = r.maxe;
+  out[1] = r.maxe / range;
+  out[2] = 20 * log10(range) - 10 * log10(mse);
+  out[3] = sqrt(mse) / range;
+  out[4] = r.mn;
+  out[5] = r.mx;
+  out[6] = r.l2;
+  if (max_err_index) *max_err_index = r.idx;
+  return PRISM_OK;
+}

@@ -21,6 +21,7 @@
 #include <condition_variable>
 #include <deque>
 #include <list>
+#include <memory>
 #include <thread>
 #include <unordered_map>
 
@@ -61,7 +62,7 @@ struct SrvRequest {
   int status = 0;
   bool done = false;
   bool hit = false;
-  SrvClock::time_point t_submit, t_done;
+  SrvClock::time_point t_submit, t_start, t_done;
   int end[4] = {0, 0, 0, 0};
   int maxlevel = 0;
 };
@@ -90,10 +91,12 @@ struct prism_server {
   std::vector<std::thread> workers;
   std::vector<cudaStream_t> streams;
   std::vector<prism_handle*> handles;
+  std::vector<std::unique_ptr<std::mutex>> slot_mu;  // held while a slot's handle is in use
   bool stop = false;
+  bool warmed = false;
   int device = 0;
   // statistics
-  std::vector<double> lat_ms;
+  std::vector<double> lat_ms, queue_ms, service_ms;
   uint64_t completed = 0, hits = 0, shared = 0, evictions = 0, failed = 0, bytes_out = 0;
   SrvClock::time_point t0;
   std::string err;
@@ -130,8 +133,10 @@ void srv_worker(prism_server* s, int slot) {
     if (s->stop) return;
     SrvRequest* r = s->queue.front();
     s->queue.pop_front();
+    r->t_start = SrvClock::now();
     const SrvField f = s->fields[r->field];  // a copy: add_field may grow the vector
     lk.unlock();
+    std::unique_lock<std::mutex> slot_lk(*s->slot_mu[slot]);
     // plane selection of the one-step retrieval (the strategy of
     // prism_progressive_step from no planes, in absolute terms)
     int begin[4] = {0, 0, 0, 0}, end[4] = {0, 0, 0, 0}, maxlevel = 4;
@@ -214,6 +219,7 @@ void srv_worker(prism_server* s, int slot) {
           }
       }
     }
+    slot_lk.unlock();
     r->status = rc;
     std::copy(end, end + 4, r->end);
     r->maxlevel = maxlevel;
@@ -224,6 +230,8 @@ void srv_worker(prism_server* s, int slot) {
       ++s->completed;
       s->bytes_out += f.value_bytes;
       s->lat_ms.push_back(std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count());
+      s->queue_ms.push_back(std::chrono::duration<double, std::milli>(r->t_start - r->t_submit).count());
+      s->service_ms.push_back(std::chrono::duration<double, std::milli>(r->t_done - r->t_start).count());
     }
     s->cv_done.notify_all();
   }
@@ -253,6 +261,15 @@ int prism_server_create(uint64_t hbm_budget, int slots, prism_server** out) {
     }
     s->streams.push_back(st);
     s->handles.push_back(h);
+    s->slot_mu.emplace_back(new std::mutex());
+  }
+  // keep freed reconstruction memory in the stream-ordered pool instead of
+  // returning it to the driver at every synchronisation (this process's
+  // default pool only)
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, s->device) == cudaSuccess) {
+    uint64_t keep = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
   }
   for (int i = 0; i < slots; ++i) s->workers.emplace_back(srv_worker, s, i);
   *out = s;
@@ -301,6 +318,19 @@ int prism_server_add_field(prism_server* s, const void* container, uint64_t size
     s->used -= size;
     return PRISM_ERR_CUDA;
   }
+  // size every slot's workspace for this field now, so that no request grows
+  // it (a cudaFree of the old workspace would stall the whole device); a
+  // slot's mutex keeps its worker off the handle meanwhile
+  for (size_t i = 0; i < s->handles.size(); ++i) {
+    std::lock_guard<std::mutex> slk(*s->slot_mu[i]);
+    prism_handle* h = s->handles[i];
+    if (ensure_common(h, g) != PRISM_OK || h->zero_anchors.ensure(g.anchors * 8 + 64) != cudaSuccess) {
+      lk.lock();
+      s->used -= size;
+      cudaFree(f.d_cont);
+      return PRISM_ERR_NOMEM;
+    }
+  }
   lk.lock();
   s->fields.push_back(f);
   *field_id = (int)s->fields.size() - 1;
@@ -316,6 +346,17 @@ int prism_server_submit(prism_server* s, int field_id, double target_error, void
   if (field_id < 0 || field_id >= (int)s->fields.size()) {
     delete r;
     return PRISM_ERR_ARG;
+  }
+  if (!s->warmed) {
+    // Map the reconstruction part of the budget into the stream-ordered pool
+    // once, so that cache misses sub-allocate instead of growing the pool
+    // (a fresh mapping of a GB-sized entry costs tens of milliseconds).
+    s->warmed = true;
+    const uint64_t room = s->budget > s->used + s->reserved ? s->budget - s->used - s->reserved : 0;
+    void* p = nullptr;
+    if (room > 0 && cudaMallocAsync(&p, room, s->streams[0]) == cudaSuccess) cudaFreeAsync(p, s->streams[0]);
+    cudaStreamSynchronize(s->streams[0]);
+    cudaGetLastError();  // a refused warm-up only costs speed
   }
   r->id = s->next_id++;
   r->field = field_id;
@@ -348,6 +389,15 @@ int prism_server_wait(prism_server* s, uint64_t request_id, double* latency_ms, 
   return rc;
 }
 
+int prism_server_poll(prism_server* s, uint64_t request_id, int* done) {
+  if (!s || !done) return PRISM_ERR_ARG;
+  std::lock_guard<std::mutex> lk(s->m);
+  auto it = s->reqs.find(request_id);
+  if (it == s->reqs.end()) return PRISM_ERR_ARG;
+  *done = it->second->done ? 1 : 0;
+  return PRISM_OK;
+}
+
 int prism_server_stats_get(prism_server* s, prism_server_stats* out, int reset) {
   if (!s || !out) return PRISM_ERR_ARG;
   std::lock_guard<std::mutex> lk(s->m);
@@ -362,19 +412,27 @@ int prism_server_stats_get(prism_server* s, prism_server_stats* out, int reset) 
   out->bytes_reserved = s->reserved;
   out->bytes_peak = s->peak;
   out->elapsed_s = std::chrono::duration<double>(SrvClock::now() - s->t0).count();
-  if (!s->lat_ms.empty()) {
-    std::vector<double> v = s->lat_ms;
+  auto pct = [](std::vector<double> v, double p) {
+    if (v.empty()) return 0.0;
     std::sort(v.begin(), v.end());
-    auto q = [&](double p) { return v[std::min(v.size() - 1, (size_t)(p * (v.size() - 1) + 0.5))]; };
-    out->p50_ms = q(0.50);
-    out->p99_ms = q(0.99);
+    return v[std::min(v.size() - 1, (size_t)(p * (v.size() - 1) + 0.5))];
+  };
+  if (!s->lat_ms.empty()) {
+    out->p50_ms = pct(s->lat_ms, 0.50);
+    out->p99_ms = pct(s->lat_ms, 0.99);
     double sum = 0;
-    for (double x : v) sum += x;
-    out->mean_ms = sum / v.size();
-    out->max_ms = v.back();
+    for (double x : s->lat_ms) sum += x;
+    out->mean_ms = sum / s->lat_ms.size();
+    out->max_ms = pct(s->lat_ms, 1.0);
+    out->queue_p50_ms = pct(s->queue_ms, 0.50);
+    out->queue_p99_ms = pct(s->queue_ms, 0.99);
+    out->service_p50_ms = pct(s->service_ms, 0.50);
+    out->service_p99_ms = pct(s->service_ms, 0.99);
   }
   if (reset) {
     s->lat_ms.clear();
+    s->queue_ms.clear();
+    s->service_ms.clear();
     s->completed = s->hits = s->shared = s->evictions = s->failed = s->bytes_out = 0;
     s->t0 = SrvClock::now();
   }

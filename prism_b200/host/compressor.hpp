@@ -80,8 +80,8 @@ class Compressor {
     check(prism_progressive_step(prog_, target_error, d_values, stream));
     time_total = t.stop();
   }
-  void progressive_state(int begin[4], int end[4], int* maxlevel) const {
-    prism_progressive_state(prog_, begin, end, maxlevel, nullptr);
+  void progressive_state(int begin[4], int end[4], int* maxlevel, uint64_t* loaded = nullptr) const {
+    prism_progressive_state(prog_, begin, end, maxlevel, loaded);
   }
 
  private:

@@ -30,23 +30,19 @@ bool write_file(const std::string& path, const void* p, size_t n) {
   return true;
 }
 
-// statistic (analyze.hpp:5-73): max error, max relative error, PSNR, NRMSE
+// statistic (analyze.hpp:5-73) on the GPU: max error, max relative error,
+// PSNR, NRMSE of d_dat against d_ori (both on the device)
 template <typename T>
-void statistic(const T* ori, const T* dat, size_t n) {
-  double mx = ori[0], mn = ori[0], max_err = 0, l2 = 0;
-  size_t idx = 0;
-  for (size_t i = 0; i < n; ++i) {
-    double o = ori[i];
-    mx = o > mx ? o : mx;
-    mn = o < mn ? o : mn;
-    double e = std::fabs((double)dat[i] - o);
-    if (max_err < e) { max_err = e; idx = i; }
-    l2 += e * e;
+void statistic(prism_handle* h, const T* d_ori, const T* d_dat, size_t n, cudaStream_t st) {
+  double s[7];
+  uint64_t idx = 0;
+  if (prism_statistics(h, d_ori, d_dat, sizeof(T), n, s, &idx, st) != PRISM_OK) {
+    std::cerr << "statistics failed: " << prism_last_error(h) << std::endl;
+    return;
   }
-  double range = mx - mn, mse = l2 / n;
-  printf("  Max_E  = %.15lf, idx = %d\n", max_err, (int)idx);
-  printf("  Max_RE = %G\n", max_err / range);
-  printf("  PSNR = %.7lf, NRMSE = %.10G\n", 20 * log10(range) - 10 * log10(mse), sqrt(mse) / range);
+  printf("  Max_E  = %.15lf, idx = %d\n", s[0], (int)idx);
+  printf("  Max_RE = %G\n", s[1]);
+  printf("  PSNR = %.7lf, NRMSE = %.10G\n", s[2], s[3]);
 }
 
 void print_time(const char* what, size_t bytes, double ms) {
@@ -66,6 +62,15 @@ int run(prism_context* c) {
   cudaMalloc(&d_data, bytes);
   cudaMalloc(&d_cont, comp.max_compressed_size());
   std::vector<char> ori;
+  T* d_ori = nullptr;  // original on the device for --report cr
+  prism_handle* stat_h = nullptr;
+  if (c->report_cr) {
+    cudaMalloc(&d_ori, bytes);
+    prism_create(&stat_h);
+  }
+  auto upload_ori = [&]() {
+    if (d_ori && !ori.empty()) cudaMemcpy(d_ori, ori.data(), bytes, cudaMemcpyHostToDevice);
+  };
   try {
     if (c->isComp) {
       if (!read_file(c->oriFilePath, ori, bytes)) return 1;
@@ -87,6 +92,7 @@ int run(prism_context* c) {
       if (!read_file(c->cmpFilePath, cont, 0)) return 1;
       cudaMemcpy(d_cont, cont.data(), cont.size(), cudaMemcpyHostToDevice);
       if (c->report_cr && ori.empty() && !read_file(c->oriFilePath, ori, bytes)) return 1;
+      upload_ori();
       std::vector<T> host(n);
       if (c->compMode && !c->target_ebs.empty()) {
         cudaMemset(d_data, 0, bytes);
@@ -94,12 +100,14 @@ int run(prism_context* c) {
           comp.decompress_progressive_pipeline(d_cont, cont.size(), d_data, c->target_ebs[i], st);
           if (c->report_time) print_time("itotal", bytes, comp.time_total);
           if (c->report_cr) {
-            cudaMemcpy(host.data(), d_data, bytes, cudaMemcpyDeviceToHost);
-            statistic<T>((const T*)ori.data(), host.data(), n);
+            statistic<T>(stat_h, d_ori, d_data, n, st);
             int b[4], e[4], ml;
-            comp.progressive_state(b, e, &ml);
-            printf("  Planes loaded per level: %d %d %d %d\n--------------------------------------\n", e[0], e[1],
-                   e[2], e[3]);
+            uint64_t loaded = 0;
+            comp.progressive_state(b, e, &ml, &loaded);
+            // calculate_accumulate_size (analyze.hpp:118-159)
+            printf("  Planes loaded per level: %d %d %d %d\n", e[0], e[1], e[2], e[3]);
+            printf("  Total Retrieved size: %llu (%lf%%)\n", (unsigned long long)loaded, 100.0 * loaded / bytes);
+            printf("  Bit rate: %lf\n--------------------------------------\n", sizeof(T) * 8.0 * loaded / bytes);
           }
         }
       } else {
@@ -109,7 +117,7 @@ int run(prism_context* c) {
       cudaMemcpy(host.data(), d_data, bytes, cudaMemcpyDeviceToHost);
       if (!write_file(c->decFilePath, host.data(), bytes)) return 1;
       std::cout << "decompressed file written: " << c->decFilePath << '\n';
-      if (c->report_cr && !(c->compMode && !c->target_ebs.empty())) statistic<T>((const T*)ori.data(), host.data(), n);
+      if (c->report_cr && !(c->compMode && !c->target_ebs.empty())) statistic<T>(stat_h, d_ori, d_data, n, st);
     }
   } catch (const prism::Error& e) {
     std::cerr << e.what() << std::endl;
@@ -117,6 +125,8 @@ int run(prism_context* c) {
   }
   cudaFree(d_data);
   cudaFree(d_cont);
+  if (d_ori) cudaFree(d_ori);
+  if (stat_h) prism_destroy(stat_h);
   cudaStreamDestroy(st);
   return 0;
 }
