@@ -40,6 +40,10 @@ TARGETS = [1e-2, 1e-3, 1e-4, 1e-5, 1e-6]
 REL_EB = 1e-6
 SAMPLE_Z = 64  # CPU baseline slab: the first 64 z-planes
 L2_BYTES = 126 * 1024 * 1024
+# DRAM bytes (read + write) per stage launch from one Nsight Compute capture of
+# this workload (interior + edge launches of a progressive step; see
+# profiles/reconstruct_kernel_progressive_f64_384x384x256.md)
+NCU_TRAFFIC = {"reconstruct": 606.0e6 + 76.0e6}
 
 
 def measured_peak():
@@ -315,7 +319,7 @@ def run_prism(args, world, rank, local):
     achieved = alg[dom] * dom_n / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": f"{peak_kind} copy bandwidth",
-                "traffic": None, "bytes_per_launch": alg[dom], "launches": dom_n,
+                "traffic": NCU_TRAFFIC.get(dom), "bytes_per_launch": alg[dom], "launches": dom_n,
                 "ms_per_launch": dom_ms / max(dom_n, 1)}
     stages = {k: {"ms_per_step": v[0] / args.steps, "launches_per_step": v[1] / args.steps,
                   "GBps": (alg[k] * v[1] / (v[0] / 1e3) / 1e9) if v[0] > 0 and alg[k] else None}
