@@ -165,3 +165,47 @@ def uneven_mix(count=64, seed=47, lo=32, hi=2048, cap3=512 ** 3):
         e = [max(lo, int(v)) for v in ext] + [1] * (3 - d)
         out.append(("sinusoid" if i % 2 == 0 else "grf", (e[0], e[1], e[2])))
     return out
+
+
+def device_voronoi(shape, dtype, seed, device="cuda", cells=64, zero_frac=0.3, spike_frac=1e-3, spike_amp=1e3,
+                   slab=16):
+    """Device version of `voronoi` (same construction, torch RNG)."""
+    import torch
+    rng = np.random.default_rng(seed)
+    nz, ny, nx = shape
+    seeds = torch.tensor(rng.uniform(0.0, 1.0, size=(cells, 3)) * np.array([nz, ny, nx]), device=device,
+                         dtype=torch.float32)
+    coef = rng.normal(0.0, 1.0, size=(cells, 10))
+    coef[rng.uniform(0.0, 1.0, cells) < zero_frac] = 0.0
+    coef = torch.tensor(coef, device=device, dtype=torch.float32)
+    tdt = torch.float32 if np.dtype(dtype) == np.float32 else torch.float64
+    out = torch.empty(shape, device=device, dtype=tdt)
+    y = (torch.arange(ny, device=device, dtype=torch.float32) / ny)[None, :, None]
+    x = (torch.arange(nx, device=device, dtype=torch.float32) / nx)[None, None, :]
+    sy = torch.arange(ny, device=device, dtype=torch.float32)[None, :, None]
+    sx = torch.arange(nx, device=device, dtype=torch.float32)[None, None, :]
+    for z0 in range(0, nz, slab):
+        z1 = min(nz, z0 + slab)
+        sz = torch.arange(z0, z1, device=device, dtype=torch.float32)[:, None, None]
+        best = torch.full((z1 - z0, ny, nx), float("inf"), device=device)
+        owner = torch.zeros((z1 - z0, ny, nx), device=device, dtype=torch.long)
+        for c in range(cells):
+            d = (sz - seeds[c, 0]) ** 2 + (sy - seeds[c, 1]) ** 2 + (sx - seeds[c, 2]) ** 2
+            m = d < best
+            best = torch.where(m, d, best)
+            owner = torch.where(m, torch.full_like(owner, c), owner)
+        zz = sz / nz
+        cc = coef[owner]
+        v = (cc[..., 0] + cc[..., 1] * x + cc[..., 2] * y + cc[..., 3] * zz + cc[..., 4] * x * x
+             + cc[..., 5] * y * y + cc[..., 6] * zz * zz + cc[..., 7] * x * y + cc[..., 8] * y * zz
+             + cc[..., 9] * x * zz)
+        out[z0:z1] = v.to(tdt)
+    n = out.numel()
+    nspk = int(round(n * spike_frac))
+    if nspk:
+        g = torch.Generator(device=device)
+        g.manual_seed(int(seed))
+        idx = torch.randint(0, n, (nspk,), device=device, generator=g)
+        sign = torch.where(torch.rand(nspk, device=device, generator=g) < 0.5, -1.0, 1.0)
+        out.view(-1)[idx] = (sign * spike_amp).to(tdt)
+    return out
