@@ -103,7 +103,10 @@ int prism_decompress_host(prism_handle* h, const void* h_container, uint64_t siz
 /* Progressive retrieval of a negabinary (-prog) container that stays resident
  * on the device (the caller keeps d_container alive).  Each step picks the
  * planes the target error needs, decodes only their chunks and refines the
- * values in d_values in place (the first step overwrites them). */
+ * values in d_values in place (the first step overwrites them).  A step is
+ * enqueued on `stream` and returns without waiting (the plane state stays in
+ * device memory); prism_progressive_state waits for the last step and
+ * returns PRISM_ERR_CORRUPT if any step met a corrupt chunk. */
 int prism_progressive_open(prism_handle* h, const void* d_container, uint64_t size, int dtype_size,
                            uint32_t nx, uint32_t ny, uint32_t nz, int mode, double bound,
                            prism_prog** out);

@@ -247,7 +247,8 @@ class Compressor:
 
 class Progressive:
     """decompress_progressive_pipeline as a resident object: each step refines
-    the reconstruction in place (compressor.cu:166-190)."""
+    the reconstruction in place (compressor.cu:166-190).  Steps are enqueued
+    on the current stream without waiting; state() waits and reports errors."""
 
     def __init__(self, comp: Compressor, d_cont):
         torch = _torch()
@@ -267,10 +268,11 @@ class Progressive:
         return self.values
 
     def state(self):
+        """Plane state after the last step (waits for it; raises on a corrupt chunk)."""
         b = (C.c_int * 4)()
         e = (C.c_int * 4)()
         ml = C.c_int()
-        lib().prism_progressive_state(self.ptr, b, e, C.byref(ml), None)
+        self.comp.h.check(lib().prism_progressive_state(self.ptr, b, e, C.byref(ml), None), "prism_progressive_state")
         return list(b), list(e), ml.value
 
     def close(self):

@@ -199,8 +199,7 @@ int prism_file_step(prism_file* f, double target_error, void* d_values, void* st
   }
   rc = prism_progressive_step(f->prog, target_error, d_values, stream);
   if (rc) return rc;
-  prism_progressive_state(f->prog, f->begin, f->end, &f->maxlevel, nullptr);
-  return PRISM_OK;
+  return prism_progressive_state(f->prog, f->begin, f->end, &f->maxlevel, nullptr);
 }
 
 int prism_file_info(const prism_file* f, uint64_t* file_bytes, uint64_t* bytes_read, int end[4]) {

@@ -363,10 +363,13 @@ struct LevelSweep {
   // The reconstruction keeps each point's code, already converted with
   // from_int, in the point's own window slot until the point is predicted
   // (no prediction reads a point of its own or a later stage).
-  __device__ __forceinline__ void emit(int wi, T pred) const {
+  // Compression keeps the codes of the tile's own 16^3 points only (the
+  // codes of the shared faces belong to the neighbouring tiles).
+  __device__ __forceinline__ void emit(int wi, const int c[3], T pred) const {
     if (COMPRESS) {
       T rec;
-      cw[wi] = quantize(win[wi], pred, ebr, ebx2, &rec);
+      const int32_t code = quantize(win[wi], pred, ebr, ebx2, &rec);
+      if ((c[0] | c[1] | c[2]) < 16) cw[(c[2] * 16 + c[1]) * 16 + c[0]] = code;
       win[wi] = rec;
     } else {
       win[wi] = Fp<T>::fma(win[wi], ebx2, pred);
@@ -395,7 +398,7 @@ struct LevelSweep {
       c[A2] = U * (k2 * ST2 + OF2);
       if (!pred_ok(c, exclusive)) continue;
       const int wi = (c[2] * kWin + c[1]) * kWin + c[0];
-      emit(wi, line_at<T, U, AX, MD>(win + wi, order_of<U, EDGE, AX>(L, c[AX]), nat));
+      emit(wi, c, line_at<T, U, AX, MD>(win + wi, order_of<U, EDGE, AX>(L, c[AX]), nat));
     }
     if (SYNC) __syncthreads();
   }
@@ -413,7 +416,7 @@ struct LevelSweep {
       c[P2] = 2 * U * k2 + U;
       if (!pred_ok(c, false)) continue;
       const int wi = (c[2] * kWin + c[1]) * kWin + c[0];
-      emit(wi, face_at<T, U, P1, P2>(win + wi, order_of<U, EDGE, P1>(L, c[P1]), order_of<U, EDGE, P2>(L, c[P2]),
+      emit(wi, c, face_at<T, U, P1, P2>(win + wi, order_of<U, EDGE, P1>(L, c[P1]), order_of<U, EDGE, P2>(L, c[P2]),
                                       nat));
     }
     if (SYNC) __syncthreads();
@@ -425,7 +428,7 @@ struct LevelSweep {
       int c[3] = {2 * U * (i % N) + U, 2 * U * ((i / N) % N) + U, 2 * U * (i / (N * N)) + U};
       if (!pred_ok(c, exclusive)) continue;
       const int wi = (c[2] * kWin + c[1]) * kWin + c[0];
-      emit(wi, cube_at<T, U>(win + wi, order_of<U, EDGE, 0>(L, c[0]), order_of<U, EDGE, 1>(L, c[1]),
+      emit(wi, c, cube_at<T, U>(win + wi, order_of<U, EDGE, 0>(L, c[0]), order_of<U, EDGE, 1>(L, c[1]),
                              order_of<U, EDGE, 2>(L, c[2]), nat));
     }
     __syncthreads();
@@ -577,13 +580,13 @@ __device__ __forceinline__ uint64_t slot_of(const G& g, const TileFrame& f, cons
   return lm_slot(g, lv, (uint64_t)f.gs[0] + x, (uint64_t)f.gs[1] + y, (uint64_t)f.gs[2] + z);
 }
 
-// Shared memory of a compression tile: the value window, the codes in the
-// same shape and the row table (~61 KB for double, ~42 KB for float).
+// Shared memory of a compression tile: the value window and the codes of the
+// tile's own points (~55 KB for double, so four tiles fit an SM; ~36 KB for
+// float).
 template <class T>
 struct CompressSmem {
   T win[kWinVol];
-  int32_t cw[kWinVol];
-  uint64_t rows[kWin * kWin];
+  int32_t cw[16 * 16 * 16];  // codes of the tile's own points
   PredParams<T> p;
 };
 
@@ -612,7 +615,6 @@ __device__ __forceinline__ void compress_tile(CompressSmem<T>& sm, const T* __re
   const Limits<EDGE> L{f.lim};
   const int tid = threadIdx.x;
   if (tid == 0) sm.p = *pp;
-  fill_rows(g, f, sm.rows);
   const uint64_t sy = g.nx, sz = (uint64_t)g.nx * g.ny;
   const T* base = data + (uint64_t)f.gs[0] + (uint64_t)f.gs[1] * sy + (uint64_t)f.gs[2] * sz;
   for (int b = tid; b < kWinVol; b += kPrefetch * kPredThreads) {
@@ -631,15 +633,27 @@ __device__ __forceinline__ void compress_tile(CompressSmem<T>& sm, const T* __re
   __syncthreads();
   if (tid == 0) anchors[bi[0] + (uint64_t)bi[1] * g.ax + (uint64_t)bi[2] * g.ax * g.ay] = sm.win[0];
   sweep_levels<T, true, EDGE>(sm.win, sm.cw, f.lim, f.last[2], sm.p);
-  // every non-anchor point of the tile's own region that lies in the field
-  // was emitted; the region is 16^3, plus the plane at 16 on a last tile
-  const int xs = 16 + (EDGE && f.last[0]), ys = 16 + (EDGE && f.last[1]), zs = 16 + (EDGE && f.last[2]);
-  const int total = xs * ys * zs;
-  for (int i = tid; i < total; i += kPredThreads) {
-    const int x = i % xs, y = (i / xs) % ys, z = i / (xs * ys);
+  // Every non-anchor point of the tile's own 16^3 that lies in the field was
+  // emitted (on a last tile the plane at 16 lies outside the field).  Thread
+  // t writes x = t % 16, y = t / 16 % 16 for every z; a level-0 point's slot
+  // is its row's base plus its rank in the row.
+  static_assert(kPredThreads == 256, "one thread per (x, y) column of the tile");
+  const int x = tid & 15, y = tid >> 4;
+  const uint64_t gx0 = f.gs[0], gy = (uint64_t)f.gs[1] + y;
+#pragma unroll 4
+  for (int z = 0; z < 16; ++z) {
     const int lv = win_level(x, y, z);
     if (lv == 4 || !L.in_data(x, y, z)) continue;
-    qc[slot_of(g, f, sm.rows, lv, x, y, z)] = sm.cw[(z * kWin + y) * kWin + x];
+    const uint64_t gz = (uint64_t)f.gs[2] + z;
+    uint64_t slot;
+    if (lv == 0) {
+      slot = gx0 + gy * g.leaps[0][0] + gz * g.leaps[0][1] + g.lm_prefix[0] - ((gz + 1) >> 1) * g.leaps[1][1] -
+             (uint64_t)((gz & 1) == 0) * ((gy + 1) >> 1) * g.leaps[1][0] + (uint64_t)x;
+      if (((gz | gy) & 1) == 0) slot -= (gx0 + x + 1) >> 1;
+    } else {
+      slot = lm_slot(g, lv, gx0 + x, gy, gz);
+    }
+    qc[slot] = sm.cw[(z * 16 + y) * 16 + x];
   }
 }
 

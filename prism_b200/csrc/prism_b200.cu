@@ -95,7 +95,13 @@ struct prism_handle {
   // launch (the two write disjoint tiles)
   cudaStream_t side = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
+  // device state slots of the progressive objects opened on this handle
+  // (no allocation per open); bit i of prog_used = slot i taken
+  DevBuf prog_slots;
+  uint64_t prog_used = 0;
 };
+
+constexpr int kProgSlotBytes = 128;  // StrategyState + error flag
 
 // Run `interior` on st and `edge` on the handle's side stream concurrently;
 // st waits for both before its next work.
@@ -145,6 +151,9 @@ static void prof_collect(prism_handle* h) {
   }
 }
 
+// A progressive retrieval in flight.  Its plane state and error flag live in
+// device memory, so steps are enqueued back to back without waiting; the
+// host copy of the state is refreshed when a caller asks for it.
 struct prism_prog {
   prism_handle* h;
   const uint8_t* cont;
@@ -154,7 +163,12 @@ struct prism_prog {
   int mode;
   double bound;
   int steps;
-  StrategyState state;
+  StrategyState state;          // host copy, valid when !pending
+  StrategyState* d_state = nullptr;
+  int* d_err = nullptr;         // chunk errors of every step so far
+  int slot = -1;                // slot in the handle's state block, or -1 (own allocation)
+  cudaEvent_t done = nullptr;   // recorded after the last enqueued step
+  bool pending = false;
 };
 
 static int fail(prism_handle* h, int code, const char* what, cudaError_t e = cudaSuccess) {
@@ -417,8 +431,9 @@ static int launch_encode(prism_handle* h, const uint8_t* planes, const Geometry&
   return PRISM_OK;
 }
 
+// err: where chunk errors go; null = the handle's flag, reset here
 static int launch_decode(prism_handle* h, const uint8_t* stream, uint64_t stream_bytes, const Geometry& g,
-                         const int* dbegin, const int* dend, uint8_t* planes, cudaStream_t st) {
+                         const int* dbegin, const int* dend, uint8_t* planes, cudaStream_t st, int* err = nullptr) {
   Small* s = small(h);
   const uint16_t* sizes = reinterpret_cast<const uint16_t*>(stream + 8);
   int64_t nblk = (g.chunks + kScanItems - 1) / kScanItems;
@@ -426,7 +441,10 @@ static int launch_decode(prism_handle* h, const uint8_t* stream, uint64_t stream
   scan_sizes_block<<<(unsigned)nblk, 1024, 0, st>>>(sizes, g.chunks, h->offs.as<int64_t>(), h->bsum.as<int64_t>());
   scan_block_sums<<<1, 32, 0, st>>>(h->bsum.as<int64_t>(), nblk);
   scan_add<<<(unsigned)((g.chunks + 255) / 256), 256, 0, st>>>(h->offs.as<int64_t>(), g.chunks, h->bsum.as<int64_t>());
-  CK(cudaMemsetAsync(&s->error_flag, 0, sizeof(int), st));
+  if (!err) {
+    err = &s->error_flag;
+    CK(cudaMemsetAsync(err, 0, sizeof(int), st));
+  }
   size_t smem = sizeof(DecodeShared);
   static bool attr_set = false;
   if (!attr_set) {
@@ -435,7 +453,7 @@ static int launch_decode(prism_handle* h, const uint8_t* stream, uint64_t stream
   }
   int blocks = (int)std::min<int64_t>(g.chunks, (int64_t)h->sm_count * 8);
   zbpc_decode_kernel<<<blocks, kZThreads, smem, st>>>(stream, stream_bytes, h->offs.as<int64_t>(), g, planes,
-                                                      dbegin, dend, &s->error_flag);
+                                                      dbegin, dend, err);
   prof_end(h, kStDecode, st);
   h->launches += 4;
   CK(cudaGetLastError());
@@ -561,7 +579,7 @@ int prism_create(prism_handle** out) {
 void prism_destroy(prism_handle* h) {
   if (!h) return;
   DevBuf* bufs[] = {&h->qc, &h->planes, &h->status, &h->offs, &h->bsum, &h->part, &h->wins, &h->ranges,
-                    &h->anchors, &h->small, &h->dev_in, &h->dev_out, &h->zero_anchors};
+                    &h->anchors, &h->small, &h->dev_in, &h->dev_out, &h->zero_anchors, &h->prog_slots};
   for (DevBuf* b : bufs) b->release();
   for (int i = 0; i < kStCount; ++i)
     for (int j = 0; j < 2; ++j)
@@ -711,8 +729,34 @@ int prism_progressive_open(prism_handle* h, const void* d_container, uint64_t si
   p->steps = 0;
   memset(&p->state, 0, sizeof(p->state));
   p->state.maxlevel = 4;
+  static_assert(sizeof(StrategyState) + sizeof(int) <= kProgSlotBytes, "progressive slot too small");
+  cudaError_t e = cudaSuccess;
+  if (!h->prog_slots.p) e = h->prog_slots.ensure(64 * kProgSlotBytes);
+  int slot = -1;
+  for (int i = 0; i < 64 && e == cudaSuccess; ++i)
+    if (!((h->prog_used >> i) & 1)) { slot = i; break; }
+  if (e == cudaSuccess && slot >= 0) {
+    h->prog_used |= 1ull << slot;
+    p->slot = slot;
+    p->d_state = reinterpret_cast<StrategyState*>(h->prog_slots.as<unsigned char>() + slot * kProgSlotBytes);
+    p->d_err = reinterpret_cast<int*>(reinterpret_cast<unsigned char*>(p->d_state) + sizeof(StrategyState));
+  } else if (e == cudaSuccess) {  // more than 64 open at once on one handle
+    e = cudaMalloc((void**)&p->d_state, kProgSlotBytes);
+    p->d_err = reinterpret_cast<int*>(reinterpret_cast<unsigned char*>(p->d_state) + sizeof(StrategyState));
+  }
+  // the device state is initialised by the first step, on its stream
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->done, cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    prism_progressive_close(p);
+    return fail(h, PRISM_ERR_CUDA, "progressive state", e);
+  }
   *out = p;
   return PRISM_OK;
+}
+
+__global__ void prog_init_kernel(StrategyState* st, int* err) {
+  if (threadIdx.x < 4) { st->begin[threadIdx.x] = 0; st->end[threadIdx.x] = 0; }
+  if (threadIdx.x == 0) { st->maxlevel = 4; *err = 0; }
 }
 
 template <class T>
@@ -726,24 +770,29 @@ static int progressive_step_t(prism_prog* p, double target, T* values, cudaStrea
   const uint8_t* tr = p->cont + (p->size - g.header_size);
   bool first = p->steps == 0;
   CK(cudaMemcpyAsync(&s->range, tr + 8, sizeof(double), cudaMemcpyDeviceToDevice, st));
-  CK(cudaMemcpyAsync(&s->sstate, &p->state, sizeof(StrategyState), cudaMemcpyHostToDevice, st));
-  // strategy (findStrategy_h) from the container's cumulative plane sizes
+  StrategyState* ds = p->d_state;
+  if (first) {  // no planes loaded, all levels, no errors
+    prog_init_kernel<<<1, 32, 0, st>>>(ds, p->d_err);
+    h->launches += 1;
+  }
+  // strategy (findStrategy_h) from the container's cumulative plane sizes;
+  // it advances the object's device state in place
   const uint64_t* csbp = reinterpret_cast<const uint64_t*>(tr + 16);
   prof_begin(h, kStStrategy, st);
   strategy_search_kernel<<<33, 1024, 0, st>>>(csbp, p->mode, p->bound, target, &s->range, s->sblk);
-  strategy_finish_kernel<<<1, 32, 0, st>>>(s->sblk, p->mode, p->bound, target, &s->range, &s->sstate);
+  strategy_finish_kernel<<<1, 32, 0, st>>>(s->sblk, p->mode, p->bound, target, &s->range, ds);
   prof_end(h, kStStrategy, st);
   h->launches += 3;
   // parameters with maxlevel from the strategy
   params_kernel<T><<<1, 32, 0, st>>>(p->mode, p->bound, &s->range, alpha_of(p->mode == 1 ? p->bound : 0.0), nullptr,
                                      0, tr, 4, reinterpret_cast<PredParams<T>*>(s->params), nullptr, &s->eb);
-  CK(cudaMemcpyAsync(&reinterpret_cast<PredParams<T>*>(s->params)->maxlevel, &s->sstate.maxlevel, sizeof(int),
+  CK(cudaMemcpyAsync(&reinterpret_cast<PredParams<T>*>(s->params)->maxlevel, &ds->maxlevel, sizeof(int),
                      cudaMemcpyDeviceToDevice, st));
   CK(cudaMemsetAsync(h->planes.p, 0, g.aligned_size, st));
-  rc = launch_decode(h, p->cont, p->size - g.header_size, g, s->sstate.begin, s->sstate.end,
-                     h->planes.as<uint8_t>(), st);
+  rc = launch_decode(h, p->cont, p->size - g.header_size, g, ds->begin, ds->end, h->planes.as<uint8_t>(), st,
+                     p->d_err);
   if (rc) return rc;
-  rc = launch_inverse(h, h->planes.as<uint8_t>(), g, 1 /*NB*/, s->sstate.begin, s->sstate.end, h->qc.as<int32_t>(), st);
+  rc = launch_inverse(h, h->planes.as<uint8_t>(), g, 1 /*NB*/, ds->begin, ds->end, h->qc.as<int32_t>(), st);
   if (rc) return rc;
   prof_begin(h, kStReconstruct, st);
   if (first) {
@@ -756,10 +805,25 @@ static int progressive_step_t(prism_prog* p, double target, T* values, cudaStrea
   }
   if (rc) return rc;
   prof_end(h, kStReconstruct, st);
-  CK(cudaMemcpyAsync(&p->state, &s->sstate, sizeof(StrategyState), cudaMemcpyDeviceToHost, st));
-  rc = finish(h, st);
-  if (rc) return rc;
+  CK(cudaEventRecord(p->done, st));
+  p->pending = true;
   p->steps++;
+  return PRISM_OK;
+}
+
+// Wait for the last enqueued step, refresh the host state and report the
+// device-side errors of the steps so far.
+static int progressive_sync(prism_prog* p) {
+  prism_handle* h = p->h;
+  if (!p->pending) return PRISM_OK;
+  CK(cudaEventSynchronize(p->done));
+  int err = 0;
+  CK(cudaMemcpy(&p->state, p->d_state, sizeof(StrategyState), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(&err, p->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  p->pending = false;
+  prof_collect(h);
+  if (err == 2) return fail(h, PRISM_ERR_CORRUPT, "corrupt lossless chunk");
+  if (err) return fail(h, PRISM_ERR_TIMEOUT, "device wait exceeded its limit");
   return PRISM_OK;
 }
 
@@ -770,8 +834,10 @@ int prism_progressive_step(prism_prog* p, double target_error, void* d_values, v
   return progressive_step_t<double>(p, target_error, (double*)d_values, st);
 }
 
-int prism_progressive_state(const prism_prog* p, int begin[4], int end[4], int* maxlevel, uint64_t* loaded) {
-  if (!p) return PRISM_ERR_ARG;
+int prism_progressive_state(const prism_prog* cp, int begin[4], int end[4], int* maxlevel, uint64_t* loaded) {
+  if (!cp) return PRISM_ERR_ARG;
+  prism_prog* p = const_cast<prism_prog*>(cp);  // refreshes the cached host state
+  const int rc = progressive_sync(p);
   for (int i = 0; i < 4; ++i) {
     if (begin) begin[i] = p->state.begin[i];
     if (end) end[i] = p->state.end[i];
@@ -792,10 +858,17 @@ int prism_progressive_state(const prism_prog* p, int begin[4], int end[4], int* 
       }
     *loaded = total;
   }
-  return PRISM_OK;
+  return rc;
 }
 
-void prism_progressive_close(prism_prog* p) { delete p; }
+void prism_progressive_close(prism_prog* p) {
+  if (!p) return;
+  if (p->pending) cudaEventSynchronize(p->done);
+  if (p->slot >= 0) p->h->prog_used &= ~(1ull << p->slot);
+  else if (p->d_state) cudaFree(p->d_state);
+  if (p->done) cudaEventDestroy(p->done);
+  delete p;
+}
 
 // ---- stage entry points ----
 

@@ -189,6 +189,7 @@ void srv_worker(prism_server* s, int slot) {
           prism_prog* pg = nullptr;
           if (!rc) rc = prism_progressive_open(h, f.d_cont, f.size, f.tsize, f.nx, f.ny, f.nz, f.mode, f.bound, &pg);
           if (!rc) rc = prism_progressive_step(pg, r->target, p, st);
+          if (!rc) rc = prism_progressive_state(pg, nullptr, nullptr, nullptr, nullptr);  // waits, reports errors
           if (pg) prism_progressive_close(pg);
           lk.lock();
           e->d_values = p;

@@ -79,6 +79,7 @@ class Compressor {
     Timer t(stream);
     check(prism_progressive_step(prog_, target_error, d_values, stream));
     time_total = t.stop();
+    check(prism_progressive_state(prog_, nullptr, nullptr, nullptr, nullptr));  // device-side errors of the step
   }
   void progressive_state(int begin[4], int end[4], int* maxlevel, uint64_t* loaded = nullptr) const {
     prism_progressive_state(prog_, begin, end, maxlevel, loaded);
