@@ -276,11 +276,20 @@ def run_prism(args, world, rank, local):
     value = weak_throughput(bytes_step, args.steps, world, ms_max)
 
     # ---- end-to-end through host buffers (C ABI, copies inside the region) ----
+    # Each retrieval is written out of place into one of two device buffers
+    # (output_old -> output_new, as the reference's CLI alternates them) and
+    # copied to the host on a copy stream while the next retrieval runs; a
+    # buffer is rewritten only after its copy has landed.
     h_in = torch.from_numpy(host).pin_memory()
     cap = comp.max_container_size()
     h_cont = torch.empty(cap, dtype=torch.uint8).pin_memory()
-    h_vals = torch.empty((nz, ny, nx), dtype=torch.float64).pin_memory()
+    h_vals = [torch.empty((nz, ny, nx), dtype=torch.float64).pin_memory() for _ in range(2)]
+    d_vals = [values, torch.empty_like(values)]
     d_cont2 = torch.empty(cap, dtype=torch.uint8, device="cuda")
+    copy_stream = torch.cuda.Stream()
+    landed = [torch.cuda.Event(), torch.cuda.Event()]
+    for ev in landed:
+        ev.record(copy_stream)
     size = C.c_uint64()
     st = C.c_void_p(stream.cuda_stream)
 
@@ -292,23 +301,43 @@ def run_prism(args, world, rank, local):
         ptr = C.c_void_p()
         h.check(lib.prism_progressive_open(h.ptr, C.c_void_p(d_cont2.data_ptr()), csz, 8, nx, ny, nz, P.REL,
                                            REL_EB, C.byref(ptr)), "open")
-        for t in TARGETS:
-            h.check(lib.prism_progressive_step(ptr, t, C.c_void_p(values.data_ptr()), st), "step")
-            h_vals.copy_(values, non_blocking=True)
+        prev = None
+        for i, t in enumerate(TARGETS):
+            k = i % 2
+            stream.wait_event(landed[k])
+            h.check(lib.prism_progressive_step_into(ptr, t, prev, C.c_void_p(d_vals[k].data_ptr()), st), "step")
+            copy_stream.wait_stream(stream)
+            with torch.cuda.stream(copy_stream):
+                h_vals[k].copy_(d_vals[k], non_blocking=True)
+            landed[k].record(copy_stream)
+            prev = C.c_void_p(d_vals[k].data_ptr())
+        h.check(lib.prism_progressive_state(ptr, None, None, None, None), "state")
         lib.prism_progressive_close(ptr)
-        torch.cuda.current_stream().synchronize()
         return csz
 
     for _ in range(max(1, args.warmup)):
         csz = e2e_workflow()
+    stream.wait_stream(copy_stream)
     barrier()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
         csz = e2e_workflow()
+    stream.wait_stream(copy_stream)
     e1.record(stream)
     barrier()
     e2e_value = weak_throughput(bytes_step, args.steps, world, max_over_ranks(e0.elapsed_time(e1), world))
+    # PCIe bound of the end-to-end workflow: pinned copies of the field alone
+    pcie = {}
+    for name, dst, src in (("h2d", d_in, h_in), ("d2h", h_vals[0], values)):
+        dst.copy_(src, non_blocking=True)
+        c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        c0.record(stream)
+        for _ in range(3):
+            dst.copy_(src, non_blocking=True)
+        c1.record(stream)
+        c1.synchronize()
+        pcie[name] = 3 * field_bytes / (c0.elapsed_time(c1) / 1e3) / 1e9
 
     # ---- roofline of the dominant stage ----
     peak, peak_kind = measured_peak()
@@ -359,7 +388,10 @@ def run_prism(args, world, rank, local):
                    "bytes_per_step": bytes_step, "l2": "inputs larger than L2 (302 MB field, 126 MB L2)",
                    "parallelism": f"replicas x{world}", "final_planes": state[1]},
         "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": field_bytes + csz,
-                "d2h_bytes_per_step": csz + len(TARGETS) * field_bytes},
+                "d2h_bytes_per_step": csz + len(TARGETS) * field_bytes,
+                "pcie_GBps": pcie,
+                "pcie_bound": bytes_step / max((field_bytes + csz) / pcie["h2d"],
+                                               (csz + len(TARGETS) * field_bytes) / pcie["d2h"])},
         "roofline": roofline, "stages": stages, "cpu_baseline": cpu, "gpu_launches": launches,
         "clocks": clk,
         "batched": batched, "serving": serving,

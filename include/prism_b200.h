@@ -111,6 +111,14 @@ int prism_progressive_open(prism_handle* h, const void* d_container, uint64_t si
                            uint32_t nx, uint32_t ny, uint32_t nz, int mode, double bound,
                            prism_prog** out);
 int prism_progressive_step(prism_prog* p, double target_error, void* d_values, void* stream);
+/* The same step out of place, as decompress_progressive_pipeline(config,
+ * output_old, output_new, ...) (include/compressor.hpp:80-81,
+ * src/prism.cu:112-138): reads the previous step's values from d_prev
+ * (ignored by the first step; may equal d_out) and writes the refined values
+ * to d_out.  Alternating two buffers lets the caller copy one step's result
+ * to the host while the next step runs. */
+int prism_progressive_step_into(prism_prog* p, double target_error, const void* d_prev, void* d_out,
+                                void* stream);
 /* begin/end/maxlevel after the last step; loaded = payload bytes of the
  * planes selected so far (calculate_accumulate_size, analyze.hpp:118-159). */
 int prism_progressive_state(const prism_prog* p, int begin[4], int end[4], int* maxlevel,

@@ -62,6 +62,7 @@ def lib():
         l.prism_decompress_host.argtypes = [vp, vp, u64, i32, u32, u32, u32, i32, dbl, vp, vp]
         l.prism_progressive_open.argtypes = [vp, vp, u64, i32, u32, u32, u32, i32, dbl, C.POINTER(vp)]
         l.prism_progressive_step.argtypes = [vp, dbl, vp, vp]
+        l.prism_progressive_step_into.argtypes = [vp, dbl, vp, vp, vp]
         l.prism_progressive_state.argtypes = [vp, vp, vp, vp, vp]
         l.prism_progressive_close.argtypes = [vp]
         l.prism_extrema.argtypes = [vp, vp, i32, u64, C.POINTER(dbl), vp]
@@ -113,6 +114,7 @@ EXPORTED = [
     "prism_batch_destroy", "prism_server_create", "prism_server_add_field", "prism_server_submit",
     "prism_server_wait", "prism_server_stats_get", "prism_server_destroy", "prism_statistics", "prism_server_poll",
     "prism_file_save", "prism_file_open", "prism_file_step", "prism_file_info", "prism_file_close",
+    "prism_progressive_step_into",
 ]
 
 STAGES = ["extrema", "autotune", "predict", "shuffle", "encode", "trailer", "strategy", "decode",
@@ -266,6 +268,16 @@ class Progressive:
         rc = lib().prism_progressive_step(self.ptr, target, C.c_void_p(self.values.data_ptr()), _stream(torch))
         self.comp.h.check(rc, "prism_progressive_step")
         return self.values
+
+    def step_into(self, target, prev, out):
+        """The step out of place (output_old -> output_new, compressor.hpp:80):
+        reads the previous step's values from `prev` (None on the first step)
+        and writes the refined values to `out`."""
+        torch = _torch()
+        rc = lib().prism_progressive_step_into(self.ptr, target, C.c_void_p(prev.data_ptr()) if prev is not None
+                                               else None, C.c_void_p(out.data_ptr()), _stream(torch))
+        self.comp.h.check(rc, "prism_progressive_step_into")
+        return out
 
     def state(self):
         """Plane state after the last step (waits for it; raises on a corrupt chunk)."""

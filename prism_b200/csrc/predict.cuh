@@ -556,46 +556,55 @@ __device__ __forceinline__ uint64_t lm_slot(const G& g, int level, uint64_t gx, 
   return gid;
 }
 
-// Row table: rows[(z*17 + y)] = level-0 slot of window point (0, y, z) minus
-// the x-dependent part, so that a level-0 point's slot is
-// rows[row] + x - (y, z both even ? (x + 1) / 2 : 0) (x, gs[0] even).
-template <class G>
-__device__ __forceinline__ void fill_rows(const G& g, const TileFrame& f, uint64_t* rows) {
-  for (int r = threadIdx.x; r < kWin * kWin; r += kPredThreads) {
-    const uint64_t gy = f.gs[1] + r % kWin, gz = f.gs[2] + r / kWin;
-    uint64_t base = (uint64_t)f.gs[0] + gy * g.leaps[0][0] + gz * g.leaps[0][1] + g.lm_prefix[0] -
-                    ((gz + 1) >> 1) * g.leaps[1][1] - (uint64_t)((gz & 1) == 0) * ((gy + 1) >> 1) * g.leaps[1][0];
-    if (((gz | gy) & 1) == 0) base -= f.gs[0] >> 1;
-    rows[r] = base;
-  }
+// Row table of a tile: for each level l and each window row (y, z) whose
+// coordinates are multiples of 2^l, the level-major slot of the row's level-l
+// point at x = 0 (lm_slot with gx = gs[0]).  Along a row the level-l points
+// are consecutive slots: writing x' = x >> l, a point's slot is
+// rows[row] + x' when (y >> l) or (z >> l) is odd, else rows[row] + x' / 2
+// (x' is then odd; gs[0] >> l is even, which makes the x part split off).
+// Level l has (16 >> l) + 1 window coordinates per axis: 17^2 + 9^2 + 5^2 +
+// 3^2 = 404 rows.
+constexpr int kRowTable = 404;
+
+__device__ __forceinline__ int row_of(int l, int y, int z) {
+  const int w = (16 >> l) + 1;
+  const int off = l == 0 ? 0 : (l == 1 ? 289 : (l == 2 ? 370 : 395));
+  return off + (z >> l) * w + (y >> l);
 }
 
 template <class G>
-__device__ __forceinline__ uint64_t slot_of(const G& g, const TileFrame& f, const uint64_t* rows, int lv,
-                                            int x, int y, int z) {
-  if (lv == 0) {
-    const int row = z * kWin + y;
-    return rows[row] + (uint64_t)x - ((((y | z) & 1) == 0) ? (uint64_t)((x + 1) >> 1) : 0);
+__device__ __forceinline__ void fill_rows(const G& g, const TileFrame& f, uint64_t* rows) {
+  for (int r = threadIdx.x; r < kRowTable; r += kPredThreads) {
+    const int l = r < 289 ? 0 : (r < 370 ? 1 : (r < 395 ? 2 : 3));
+    const int w = (16 >> l) + 1, k = r - (l == 0 ? 0 : (l == 1 ? 289 : (l == 2 ? 370 : 395)));
+    const int y = (k % w) << l, z = (k / w) << l;
+    rows[r] = lm_slot(g, l, (uint64_t)f.gs[0], (uint64_t)f.gs[1] + y, (uint64_t)f.gs[2] + z);
   }
-  return lm_slot(g, lv, (uint64_t)f.gs[0] + x, (uint64_t)f.gs[1] + y, (uint64_t)f.gs[2] + z);
+}
+
+// Slot of window point (x, y, z) of level lv (0..3) from the row table.
+__device__ __forceinline__ uint64_t slot_of(const uint64_t* rows, int lv, int x, int y, int z) {
+  const int ee = (((y | z) >> lv) & 1) == 0;
+  return rows[row_of(lv, y, z)] + (uint64_t)((x >> lv) >> ee);
 }
 
 // Shared memory of a compression tile: the value window and the codes of the
 // tile's own points (~55 KB for double, so four tiles fit an SM; ~36 KB for
-// float).
+// float).  The row table takes the window's place once the sweeps are done.
 template <class T>
 struct CompressSmem {
-  T win[kWinVol];
+  T win[kWinVol];  // after the sweeps: the row table
   int32_t cw[16 * 16 * 16];  // codes of the tile's own points
   PredParams<T> p;
 };
+static_assert(sizeof(float) * kWinVol >= sizeof(uint64_t) * kRowTable, "row table fits the window");
 
 // Shared memory of a reconstruction tile: the window (codes travel in the
-// window slots) and the row table (~42 KB for double, ~22 KB for float).
+// window slots) and the row table (~43 KB for double, ~23 KB for float).
 template <class T>
 struct ReconSmem {
   T win[kWinVol];
-  uint64_t rows[kWin * kWin];
+  uint64_t rows[kRowTable];
   PredParams<T> p;
 };
 
@@ -634,26 +643,16 @@ __device__ __forceinline__ void compress_tile(CompressSmem<T>& sm, const T* __re
   if (tid == 0) anchors[bi[0] + (uint64_t)bi[1] * g.ax + (uint64_t)bi[2] * g.ax * g.ay] = sm.win[0];
   sweep_levels<T, true, EDGE>(sm.win, sm.cw, f.lim, f.last[2], sm.p);
   // Every non-anchor point of the tile's own 16^3 that lies in the field was
-  // emitted (on a last tile the plane at 16 lies outside the field).  Thread
-  // t writes x = t % 16, y = t / 16 % 16 for every z; a level-0 point's slot
-  // is its row's base plus its rank in the row.
-  static_assert(kPredThreads == 256, "one thread per (x, y) column of the tile");
-  const int x = tid & 15, y = tid >> 4;
-  const uint64_t gx0 = f.gs[0], gy = (uint64_t)f.gs[1] + y;
-#pragma unroll 4
-  for (int z = 0; z < 16; ++z) {
+  // emitted (on a last tile the plane at 16 lies outside the field).
+  __syncthreads();
+  uint64_t* rows = reinterpret_cast<uint64_t*>(sm.win);
+  fill_rows(g, f, rows);
+  __syncthreads();
+  for (int i = tid; i < 16 * 16 * 16; i += kPredThreads) {
+    const int x = i & 15, y = (i >> 4) & 15, z = i >> 8;
     const int lv = win_level(x, y, z);
     if (lv == 4 || !L.in_data(x, y, z)) continue;
-    const uint64_t gz = (uint64_t)f.gs[2] + z;
-    uint64_t slot;
-    if (lv == 0) {
-      slot = gx0 + gy * g.leaps[0][0] + gz * g.leaps[0][1] + g.lm_prefix[0] - ((gz + 1) >> 1) * g.leaps[1][1] -
-             (uint64_t)((gz & 1) == 0) * ((gy + 1) >> 1) * g.leaps[1][0] + (uint64_t)x;
-      if (((gz | gy) & 1) == 0) slot -= (gx0 + x + 1) >> 1;
-    } else {
-      slot = lm_slot(g, lv, gx0 + x, gy, gz);
-    }
-    qc[slot] = sm.cw[(z * 16 + y) * 16 + x];
+    qc[slot_of(rows, lv, x, y, z)] = sm.cw[i];
   }
 }
 
@@ -698,7 +697,7 @@ reconstruct_kernel(const int32_t* __restrict__ qc, const T* __restrict__ anchors
       v[k] = 0;
       const int lv = win_level(x, y, z);
       if (i < kWinVol && lv < 4 && lv <= maxlevel && L.in_data(x, y, z))
-        v[k] = __ldg(qc + slot_of(g, f, sm.rows, lv, x, y, z));
+        v[k] = __ldg(qc + slot_of(sm.rows, lv, x, y, z));
     }
 #pragma unroll
     for (int k = 0; k < kPrefetch; ++k) {

@@ -80,9 +80,22 @@ struct HostResult {
 enum Stage { kStExtrema, kStAutotune, kStPredict, kStShuffle, kStEncode, kStTrailer, kStStrategy, kStDecode,
              kStInverse, kStReconstruct, kStCount };
 
+// What a progressive step publishes for the host: the plane state, the
+// error flag and the payload bytes of the planes loaded so far.
+struct ProgMirror {
+  StrategyState state;
+  int err;
+  uint64_t loaded;
+};
+
 struct prism_handle {
   DevBuf qc, planes, status, offs, bsum, part, wins, ranges, anchors, small, dev_in, dev_out, zero_anchors;
-  HostResult* host = nullptr;  // pinned
+  // Pinned host memory mapped into the device: kernels store the results the
+  // host reads (sizes, flags, parameters, progressive state) straight into
+  // it, so reading them waits only for the kernels, never behind other
+  // device-to-host copies in flight on the copy engines.
+  HostResult* host = nullptr;
+  HostResult* host_dev = nullptr;  // device alias of host
   std::string err;
   int sm_count = 148;
   uint64_t launches = 0;       // kernels launched by this handle
@@ -99,9 +112,23 @@ struct prism_handle {
   // (no allocation per open); bit i of prog_used = slot i taken
   DevBuf prog_slots;
   uint64_t prog_used = 0;
+  ProgMirror* prog_host = nullptr;  // 64 mapped mirrors, one per slot
+  ProgMirror* prog_host_dev = nullptr;
 };
 
 constexpr int kProgSlotBytes = 128;  // StrategyState + error flag
+
+static cudaError_t host_mapped(size_t bytes, void** host, void** dev) {
+  cudaError_t e = cudaHostAlloc(host, bytes, cudaHostAllocMapped);
+  if (e != cudaSuccess) return e;
+  memset(*host, 0, bytes);
+  e = cudaHostGetDevicePointer(dev, *host, 0);
+  if (e != cudaSuccess) {
+    cudaFreeHost(*host);
+    *host = nullptr;
+  }
+  return e;
+}
 
 // Run `interior` on st and `edge` on the handle's side stream concurrently;
 // st waits for both before its next work.
@@ -167,6 +194,9 @@ struct prism_prog {
   StrategyState* d_state = nullptr;
   int* d_err = nullptr;         // chunk errors of every step so far
   int slot = -1;                // slot in the handle's state block, or -1 (own allocation)
+  ProgMirror* mirror = nullptr;      // mapped host copy written by each step
+  ProgMirror* mirror_dev = nullptr;
+  uint64_t loaded = 0;          // host copy, valid when !pending
   cudaEvent_t done = nullptr;   // recorded after the last enqueued step
   bool pending = false;
 };
@@ -478,12 +508,21 @@ __global__ void trailer_kernel(uint8_t* stream, const uint64_t* padded, const Pr
   }
 }
 
+// the results of a pipeline call, stored into the handle's mapped host block
+__global__ void publish_result_kernel(const Small* __restrict__ s, HostResult* out) {
+  const int t = threadIdx.x;
+  if (t == 0) {
+    out->padded_size = s->padded_size;
+    out->error_flag = s->error_flag;
+  }
+  if (t < (int)sizeof(s->params)) out->params[t] = s->params[t];
+  if (t < 16) out->errors[t] = s->errors[t];
+}
+
 static int finish(prism_handle* h, cudaStream_t st) {
-  Small* s = small(h);
-  CK(cudaMemcpyAsync(&h->host->padded_size, &s->padded_size, sizeof(uint64_t), cudaMemcpyDeviceToHost, st));
-  CK(cudaMemcpyAsync(&h->host->error_flag, &s->error_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
-  CK(cudaMemcpyAsync(h->host->params, s->params, sizeof(s->params), cudaMemcpyDeviceToHost, st));
-  CK(cudaMemcpyAsync(h->host->errors, s->errors, sizeof(s->errors), cudaMemcpyDeviceToHost, st));
+  publish_result_kernel<<<1, 256, 0, st>>>(small(h), h->host_dev);
+  h->launches += 1;
+  CK(cudaGetLastError());
   CK(cudaStreamSynchronize(st));
   prof_collect(h);
   if (h->host->error_flag == 1) return fail(h, PRISM_ERR_TIMEOUT, "look-back wait exceeded its limit");
@@ -567,7 +606,7 @@ int prism_create(prism_handle** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, dev);
-  if (e == cudaSuccess) e = cudaMallocHost((void**)&h->host, sizeof(HostResult));
+  if (e == cudaSuccess) e = host_mapped(sizeof(HostResult), (void**)&h->host, (void**)&h->host_dev);
   if (e != cudaSuccess) {
     delete h;
     return PRISM_ERR_CUDA;
@@ -588,6 +627,7 @@ void prism_destroy(prism_handle* h) {
   if (h->fork) cudaEventDestroy(h->fork);
   if (h->join) cudaEventDestroy(h->join);
   if (h->host) cudaFreeHost(h->host);
+  if (h->prog_host) cudaFreeHost(h->prog_host);
   delete h;
 }
 
@@ -732,6 +772,8 @@ int prism_progressive_open(prism_handle* h, const void* d_container, uint64_t si
   static_assert(sizeof(StrategyState) + sizeof(int) <= kProgSlotBytes, "progressive slot too small");
   cudaError_t e = cudaSuccess;
   if (!h->prog_slots.p) e = h->prog_slots.ensure(64 * kProgSlotBytes);
+  if (e == cudaSuccess && !h->prog_host)
+    e = host_mapped(64 * sizeof(ProgMirror), (void**)&h->prog_host, (void**)&h->prog_host_dev);
   int slot = -1;
   for (int i = 0; i < 64 && e == cudaSuccess; ++i)
     if (!((h->prog_used >> i) & 1)) { slot = i; break; }
@@ -740,9 +782,12 @@ int prism_progressive_open(prism_handle* h, const void* d_container, uint64_t si
     p->slot = slot;
     p->d_state = reinterpret_cast<StrategyState*>(h->prog_slots.as<unsigned char>() + slot * kProgSlotBytes);
     p->d_err = reinterpret_cast<int*>(reinterpret_cast<unsigned char*>(p->d_state) + sizeof(StrategyState));
+    p->mirror = h->prog_host + slot;
+    p->mirror_dev = h->prog_host_dev + slot;
   } else if (e == cudaSuccess) {  // more than 64 open at once on one handle
     e = cudaMalloc((void**)&p->d_state, kProgSlotBytes);
     p->d_err = reinterpret_cast<int*>(reinterpret_cast<unsigned char*>(p->d_state) + sizeof(StrategyState));
+    if (e == cudaSuccess) e = host_mapped(sizeof(ProgMirror), (void**)&p->mirror, (void**)&p->mirror_dev);
   }
   // the device state is initialised by the first step, on its stream
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p->done, cudaEventDisableTiming);
@@ -759,8 +804,26 @@ __global__ void prog_init_kernel(StrategyState* st, int* err) {
   if (threadIdx.x == 0) { st->maxlevel = 4; *err = 0; }
 }
 
+// The state after a step, for the host: plane ranges, error flag and the
+// payload bytes of every plane loaded so far.  Steps load [previous end,
+// end), so the total is planes [0, end) of each level, a difference of the
+// trailer's cumulative sizes (calculate_accumulate_size, analyze.hpp:118-159,
+// summed over the steps).
+__global__ void prog_publish_kernel(const StrategyState* __restrict__ st, const int* __restrict__ err,
+                                    const uint64_t* __restrict__ cum, ProgMirror* out) {
+  if (threadIdx.x != 0) return;
+  uint64_t total = 0;
+  for (int i = 0; i < 4; ++i) {
+    const int e = min(st->end[i], 32);
+    if (e > 0) total += cum[i * 32 + e - 1] - (i > 0 ? cum[i * 32 - 1] : 0);
+  }
+  out->state = *st;
+  out->err = *err;
+  out->loaded = total;
+}
+
 template <class T>
-static int progressive_step_t(prism_prog* p, double target, T* values, cudaStream_t st) {
+static int progressive_step_t(prism_prog* p, double target, const T* prev, T* values, cudaStream_t st) {
   prism_handle* h = p->h;
   const Geometry& g = p->g;
   int rc = ensure_common(h, g);
@@ -800,11 +863,14 @@ static int progressive_step_t(prism_prog* p, double target, T* values, cudaStrea
                                       params_ptr<T>(h), nullptr, values, st);
   } else {
     CK(cudaMemsetAsync(h->zero_anchors.p, 0, g.anchors * sizeof(T), st));
-    rc = launch_reconstruct<T, true>(h, h->qc.as<int32_t>(), h->zero_anchors.as<T>(), g, params_ptr<T>(h), values,
+    rc = launch_reconstruct<T, true>(h, h->qc.as<int32_t>(), h->zero_anchors.as<T>(), g, params_ptr<T>(h), prev,
                                      values, st);
   }
   if (rc) return rc;
   prof_end(h, kStReconstruct, st);
+  prog_publish_kernel<<<1, 32, 0, st>>>(ds, p->d_err, csbp, p->mirror_dev);
+  h->launches += 1;
+  CK(cudaGetLastError());
   CK(cudaEventRecord(p->done, st));
   p->pending = true;
   p->steps++;
@@ -817,9 +883,14 @@ static int progressive_sync(prism_prog* p) {
   prism_handle* h = p->h;
   if (!p->pending) return PRISM_OK;
   CK(cudaEventSynchronize(p->done));
-  int err = 0;
-  CK(cudaMemcpy(&p->state, p->d_state, sizeof(StrategyState), cudaMemcpyDeviceToHost));
-  CK(cudaMemcpy(&err, p->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  const volatile ProgMirror* m = p->mirror;
+  for (int i = 0; i < 4; ++i) {
+    p->state.begin[i] = m->state.begin[i];
+    p->state.end[i] = m->state.end[i];
+  }
+  p->state.maxlevel = m->state.maxlevel;
+  const int err = m->err;
+  p->loaded = m->loaded;
   p->pending = false;
   prof_collect(h);
   if (err == 2) return fail(h, PRISM_ERR_CORRUPT, "corrupt lossless chunk");
@@ -830,8 +901,15 @@ static int progressive_sync(prism_prog* p) {
 int prism_progressive_step(prism_prog* p, double target_error, void* d_values, void* stream) {
   if (!p || !d_values || !(target_error > 0)) return PRISM_ERR_ARG;
   cudaStream_t st = (cudaStream_t)stream;
-  if (p->tsize == 4) return progressive_step_t<float>(p, target_error, (float*)d_values, st);
-  return progressive_step_t<double>(p, target_error, (double*)d_values, st);
+  if (p->tsize == 4) return progressive_step_t<float>(p, target_error, (const float*)d_values, (float*)d_values, st);
+  return progressive_step_t<double>(p, target_error, (const double*)d_values, (double*)d_values, st);
+}
+
+int prism_progressive_step_into(prism_prog* p, double target_error, const void* d_prev, void* d_out, void* stream) {
+  if (!p || !d_out || !(target_error > 0) || (!d_prev && p->steps > 0)) return PRISM_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (p->tsize == 4) return progressive_step_t<float>(p, target_error, (const float*)d_prev, (float*)d_out, st);
+  return progressive_step_t<double>(p, target_error, (const double*)d_prev, (double*)d_out, st);
 }
 
 int prism_progressive_state(const prism_prog* cp, int begin[4], int end[4], int* maxlevel, uint64_t* loaded) {
@@ -843,29 +921,19 @@ int prism_progressive_state(const prism_prog* cp, int begin[4], int end[4], int*
     if (end) end[i] = p->state.end[i];
   }
   if (maxlevel) *maxlevel = p->state.maxlevel;
-  if (loaded) {
-    // payload bytes of every plane loaded so far: steps load [previous end,
-    // end), so the total is planes [0, end) (calculate_accumulate_size,
-    // analyze.hpp:118-159, summed over the steps)
-    uint64_t cum[128];
-    const uint8_t* tr = p->cont + (p->size - p->g.header_size);
-    if (cudaMemcpy(cum, tr + 16, sizeof(cum), cudaMemcpyDeviceToHost) != cudaSuccess) return PRISM_ERR_CUDA;
-    uint64_t total = 0;
-    for (int i = 0; i < 4; ++i)
-      for (int j = 0; j < p->state.end[i] && j < 32; ++j) {
-        const int k = i * 32 + j;
-        total += cum[k] - (k > 0 ? cum[k - 1] : 0);
-      }
-    *loaded = total;
-  }
+  if (loaded) *loaded = p->loaded;
   return rc;
 }
 
 void prism_progressive_close(prism_prog* p) {
   if (!p) return;
   if (p->pending) cudaEventSynchronize(p->done);
-  if (p->slot >= 0) p->h->prog_used &= ~(1ull << p->slot);
-  else if (p->d_state) cudaFree(p->d_state);
+  if (p->slot >= 0) {
+    p->h->prog_used &= ~(1ull << p->slot);
+  } else {
+    if (p->d_state) cudaFree(p->d_state);
+    if (p->mirror) cudaFreeHost(p->mirror);
+  }
   if (p->done) cudaEventDestroy(p->done);
   delete p;
 }

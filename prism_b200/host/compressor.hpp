@@ -81,6 +81,19 @@ class Compressor {
     time_total = t.stop();
     check(prism_progressive_state(prog_, nullptr, nullptr, nullptr, nullptr));  // device-side errors of the step
   }
+  // The step out of place, with the reference's argument pair (output_old,
+  // output_new): d_old holds the previous step's values (nullptr on the first
+  // step) and d_new receives the refined ones.
+  void decompress_progressive_pipeline(const uint8_t* d_cont, uint64_t size, const T* d_old, T* d_new,
+                                       double target_error, cudaStream_t stream) {
+    double bound = cfg_.error_mode == REL ? cfg_.rel_eb : cfg_.eb;
+    if (!prog_) check(prism_progressive_open(h_, d_cont, size, sizeof(T), cfg_.x, cfg_.y, cfg_.z, cfg_.error_mode,
+                                             bound, &prog_));
+    Timer t(stream);
+    check(prism_progressive_step_into(prog_, target_error, d_old, d_new, stream));
+    time_total = t.stop();
+    check(prism_progressive_state(prog_, nullptr, nullptr, nullptr, nullptr));
+  }
   void progressive_state(int begin[4], int end[4], int* maxlevel, uint64_t* loaded = nullptr) const {
     prism_progressive_state(prog_, begin, end, maxlevel, loaded);
   }

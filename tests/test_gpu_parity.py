@@ -78,6 +78,30 @@ def test_progressive_reference_container(env, name):
     prog.close()
 
 
+@pytest.mark.parametrize("name", SMALL_PROG)
+def test_progressive_out_of_place_reference_container(env, name):
+    """Steps through two alternating buffers (output_old -> output_new, as the
+    reference's CLI runs them) give the reference's bytes and leave the
+    previous step's buffer untouched."""
+    torch, P, h = env
+    comp = P.Compressor(ctx_of(P, name), h)
+    cont = to_dev(torch, np.frombuffer(gu.raw(name, "cmp.bin"), np.uint8))
+    prog = comp.progressive(cont)
+    dg = gu.digests(name)
+    bufs = [torch.full_like(prog.values, 7.0), torch.full_like(prog.values, 7.0)]
+    prev = None
+    for i, t in enumerate(gu.CASES[name]["targets"]):
+        out = bufs[i % 2]
+        before = prev.clone() if prev is not None else None
+        prog.step_into(t, prev, out)
+        prog.state()
+        assert gu.sha(out.cpu().numpy()) == dg[f"prog{i}.bin"][1], f"step {i}"
+        if prev is not None:
+            assert torch.equal(prev, before)
+        prev = out
+    prog.close()
+
+
 RANDOM_SHAPES = [(40, 23, 17), (70, 45, 33), (129, 3, 5), (300, 41, 1), (2000, 1, 1), (16, 16, 16), (17, 17, 17),
                  (48, 48, 48)]
 
