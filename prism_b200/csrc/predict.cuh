@@ -246,6 +246,18 @@ __device__ __forceinline__ int32_t quantize(T orig, T pred, T ebr, T ebx2, T* re
 constexpr int kPredThreads = 256;
 constexpr int kPrefetch = 8;  // independent global loads in flight per thread
 
+// Asynchronous global -> shared copies (cp.async, no register staging): a
+// thread issues every copy of its window points before waiting for any, and
+// after cp.async.wait_all sees the data it copied itself.
+template <int BYTES>
+__device__ __forceinline__ void copy_async(void* smem_dst, const void* gmem_src) {
+  static_assert(BYTES == 4 || BYTES == 8, "4- or 8-byte copies");
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(gmem_src), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void copy_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
 // ---- tile sweep --------------------------------------------------------------
 //
 // Every boundary case of pred_line / pred_face / pred_cube depends only on
@@ -609,7 +621,7 @@ struct ReconSmem {
 };
 
 // Compression: data -> anchors + level-major codes (interpolation :2137-2173).
-// The window is loaded with kPrefetch independent loads per thread in flight,
+// The window is loaded with asynchronous copies, all in flight at once,
 // the 12 stages run in shared memory, and the codes of the points the tile
 // owns leave in one pass at the end.
 // One tile of the compression (the body of predict_compress_kernel and of the
@@ -626,19 +638,14 @@ __device__ __forceinline__ void compress_tile(CompressSmem<T>& sm, const T* __re
   if (tid == 0) sm.p = *pp;
   const uint64_t sy = g.nx, sz = (uint64_t)g.nx * g.ny;
   const T* base = data + (uint64_t)f.gs[0] + (uint64_t)f.gs[1] * sy + (uint64_t)f.gs[2] * sz;
-  for (int b = tid; b < kWinVol; b += kPrefetch * kPredThreads) {
-    T v[kPrefetch];
-#pragma unroll
-    for (int k = 0; k < kPrefetch; ++k) {
-      int i = b + k * kPredThreads, x, y, z;
-      win_xyz(i, x, y, z);
-      v[k] = T(0);
-      if (i < kWinVol && L.in_data(x, y, z)) v[k] = __ldg(base + x + (uint64_t)y * sy + (uint64_t)z * sz);
-    }
-#pragma unroll
-    for (int k = 0; k < kPrefetch; ++k)
-      if (b + k * kPredThreads < kWinVol) sm.win[b + k * kPredThreads] = v[k];
+#pragma unroll 4
+  for (int i = tid; i < kWinVol; i += kPredThreads) {
+    int x, y, z;
+    win_xyz(i, x, y, z);
+    if (L.in_data(x, y, z)) copy_async<sizeof(T)>(&sm.win[i], base + x + (uint64_t)y * sy + (uint64_t)z * sz);
+    else sm.win[i] = T(0);
   }
+  copy_async_wait_all();
   __syncthreads();
   if (tid == 0) anchors[bi[0] + (uint64_t)bi[1] * g.ax + (uint64_t)bi[2] * g.ax * g.ay] = sm.win[0];
   sweep_levels<T, true, EDGE>(sm.win, sm.cw, f.lim, f.last[2], sm.p);
@@ -670,7 +677,7 @@ predict_compress_kernel(const T* __restrict__ data, Geometry g, const PredParams
 // Reconstruction: anchors + codes -> values (interpolation_reverse
 // :2177-2207); PROG adds the previous values (interpolation_progressive_reverse
 // :2209-2239, shmem2global_data_progressive :1123-1147).  All codes the tile
-// can use are fetched up front with kPrefetch loads in flight per thread.
+// can use are fetched up front with asynchronous copies.
 template <class T, bool PROG, int PART>
 __global__ void __launch_bounds__(kPredThreads, PART == 0 ? 5 : 3)
 reconstruct_kernel(const int32_t* __restrict__ qc, const T* __restrict__ anchors, Geometry g,
@@ -687,24 +694,34 @@ reconstruct_kernel(const int32_t* __restrict__ qc, const T* __restrict__ anchors
   const int maxlevel = pp->maxlevel;
   if (tid == 0) sm.p = *pp;
   fill_rows(g, f, sm.rows);
-  __syncthreads();
-  for (int b = tid; b < kWinVol; b += kPrefetch * kPredThreads) {
-    int32_t v[kPrefetch];
-#pragma unroll
-    for (int k = 0; k < kPrefetch; ++k) {
-      int i = b + k * kPredThreads, x, y, z;
-      win_xyz(i, x, y, z);
-      v[k] = 0;
-      const int lv = win_level(x, y, z);
-      if (i < kWinVol && lv < 4 && lv <= maxlevel && L.in_data(x, y, z))
-        v[k] = __ldg(qc + slot_of(sm.rows, lv, x, y, z));
-    }
-#pragma unroll
-    for (int k = 0; k < kPrefetch; ++k) {
-      int i = b + k * kPredThreads;
-      if (i < kWinVol) sm.win[i] = Fp<T>::from_int(v[k]);
+  const uint64_t sy = g.nx, sz = (uint64_t)g.nx * g.ny;
+  const uint64_t base = (uint64_t)f.gs[0] + (uint64_t)f.gs[1] * sy + (uint64_t)f.gs[2] * sz;
+  if (PROG) {
+    // the previous values are read after the sweeps: start bringing the
+    // tile's rows (16 values, one or two 128-byte lines) into L2 now
+    const int y = tid & 15, z = tid >> 4;
+    if (L.in_data(0, y, z)) {
+      const T* row = old + base + (uint64_t)y * sy + (uint64_t)z * sz;
+      prefetch_l2(row);
+      if (L.in_data(15, y, z)) prefetch_l2(row + 15);
     }
   }
+  __syncthreads();
+  // each code lands in the low word of its window slot and is converted in
+  // place by the thread that copied it
+#pragma unroll 4
+  for (int i = tid; i < kWinVol; i += kPredThreads) {
+    int x, y, z;
+    win_xyz(i, x, y, z);
+    const int lv = win_level(x, y, z);
+    int32_t* dst = reinterpret_cast<int32_t*>(&sm.win[i]);
+    if (lv < 4 && lv <= maxlevel && L.in_data(x, y, z)) copy_async<4>(dst, qc + slot_of(sm.rows, lv, x, y, z));
+    else *dst = 0;
+  }
+  copy_async_wait_all();
+#pragma unroll 4
+  for (int i = tid; i < kWinVol; i += kPredThreads)
+    sm.win[i] = Fp<T>::from_int(*reinterpret_cast<const int32_t*>(&sm.win[i]));
   __syncthreads();
   if (tid < 8) {  // x_reset_scratch_data (:1027-1067): anchors at the corners
     int x = (tid & 1) * 16, y = ((tid >> 1) & 1) * 16, z = (tid >> 2) * 16;
@@ -714,8 +731,6 @@ reconstruct_kernel(const int32_t* __restrict__ qc, const T* __restrict__ anchors
   }
   __syncthreads();
   sweep_levels<T, false, EDGE>(sm.win, nullptr, f.lim, f.last[2], sm.p);
-  const uint64_t sy = g.nx, sz = (uint64_t)g.nx * g.ny;
-  const uint64_t base = (uint64_t)f.gs[0] + (uint64_t)f.gs[1] * sy + (uint64_t)f.gs[2] * sz;
   const int xs = 16 + (EDGE && f.last[0]), ys = 16 + (EDGE && f.last[1]), zs = 16 + (EDGE && f.last[2]);
   const int total = xs * ys * zs;
   for (int b = tid; b < total; b += kPrefetch * kPredThreads) {
