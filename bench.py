@@ -370,6 +370,7 @@ def run_prism(args, world, rank, local):
         dist.destroy_process_group()
     if rank != 0:
         return 0
+    comp_flags = comp.flags
     # free the single-field buffers before the batch and serving parts
     del d_in, d_cont, values, d_cont2, comp, h
     torch.cuda.empty_cache()
@@ -386,7 +387,8 @@ def run_prism(args, world, rank, local):
                    "field_bytes": field_bytes, "container_bytes": cont_bytes,
                    "compression_ratio": field_bytes / cont_bytes,
                    "bytes_per_step": bytes_step, "l2": "inputs larger than L2 (302 MB field, 126 MB L2)",
-                   "parallelism": f"replicas x{world}", "final_planes": state[1]},
+                   "parallelism": f"replicas x{world}", "final_planes": state[1],
+                   "use_md_per_level": list(comp_flags[0]), "reverse_per_level": list(comp_flags[1])},
         "e2e": {"value": e2e_value, "unit": "GB/s", "h2d_bytes_per_step": field_bytes + csz,
                 "d2h_bytes_per_step": csz + len(TARGETS) * field_bytes,
                 "pcie_GBps": pcie,

@@ -445,10 +445,229 @@ struct LevelSweep {
     }
     __syncthreads();
   }
+  // Level 0 of an interior tile, per-axis mode, by lines: a job predicts the
+  // odd points 2j+1, j in [J0, J1), of the line along AX through window point
+  // (c[P], c[Q]) = (p, q).  The line's even points come from earlier stages
+  // and every odd point reads only those, so the points of a job are
+  // independent; the even points are read once per job.  Interior orders
+  // (order_of with no limits): j = 0 quadratic from the right, j = 7
+  // quadratic from the left, cubic in between.
+  // order along an axis at odd coordinate c of an interior tile, level 0
+  static __device__ __forceinline__ int order0(int c) { return c == 1 ? 2 : (c == 15 ? 3 : 4); }
+  // line_at at point 2j+1 of a job, from the job's even values e[k] (at 2k)
+  template <bool MD>
+  __device__ __forceinline__ T job_line(const T (&e)[9], int j) const {
+    using E = Expr<T>;
+    if (j == 0) return E::quad_r(e[0], e[1], e[2]);
+    if (j == 7) return E::quad_l(e[6], e[7], e[8]);
+    return MD ? E::cubic_lambda(e[j - 1], e[j], e[j + 1], e[j + 2], nat)
+              : E::cubic_axis(e[j - 1], e[j], e[j + 1], e[j + 2], nat);
+  }
+  // the even values a job of points [J0, J1) reads along its axis
+  template <int S, int J0, int J1>
+  __device__ __forceinline__ void job_evens(int w0, T (&e)[9]) const {
+    constexpr int K0 = J0 > 0 ? J0 - 1 : 0, K1 = J1 + 2 < 9 ? J1 + 2 : 9;
+#pragma unroll
+    for (int k = K0; k < K1; ++k) e[k] = win[w0 + 2 * k * S];
+  }
+  template <int AX, int J0, int J1, bool MD = false>
+  __device__ __forceinline__ void line_job(int p, int q) const {
+    constexpr int S = kStride[AX];
+    constexpr int P = AX == 0 ? 1 : 0, Q = AX == 2 ? 1 : 2;
+    int c[3];
+    c[P] = p;
+    c[Q] = q;
+    c[AX] = 0;
+    const int w0 = (c[2] * kWin + c[1]) * kWin + c[0];
+    T e[9];
+    job_evens<S, J0, J1>(w0, e);
+#pragma unroll
+    for (int j = J0; j < J1; ++j) {
+      c[AX] = 2 * j + 1;
+      emit(w0 + (2 * j + 1) * S, c, job_line<MD>(e, j));
+    }
+  }
+  // ---- md level 0 of an interior tile by jobs along one odd axis ----------
+  // A job walks the odd points 2j+1, j in [j0, j1), of a line with window
+  // stride S, holding the line's even values E[j-1..j+2] in a sliding window
+  // (compact code: one instance serves every axis).  cwi/cs locate the
+  // points' codes in the tile's 16^3 code block; `own` tells whether the
+  // line's fixed coordinates lie in the tile's own region.
+  __device__ __forceinline__ void emit_at(int wi, int cwi, bool own, T pred) const {
+    if (COMPRESS) {
+      T rec;
+      const int32_t code = quantize(win[wi], pred, ebr, ebx2, &rec);
+      if (own) cw[cwi] = code;
+      win[wi] = rec;
+    } else {
+      win[wi] = Fp<T>::fma(win[wi], ebx2, pred);
+    }
+  }
+  // line_at (MD) along a runtime stride with an interior order
+  __device__ __forceinline__ T line_md_rt(const T* w, int S, int o) const {
+    using E = Expr<T>;
+    const T t1 = w[-S], t2 = w[S];
+    if (o == 4) return E::cubic_lambda(w[-3 * S], t1, t2, w[3 * S], nat);
+    if (o == 3) return E::quad_l(w[-3 * S], t1, t2);
+    return E::quad_r(t1, t2, w[3 * S]);
+  }
+  // KIND 0: md line points (prediction along the job axis only);
+  // KIND 1: md faces, the job axis J and a second odd axis with stride SK
+  // and order ok (face_at: both cubic -> the mean of the two lines, one cubic
+  // -> that line, neither -> the mean; add() is commutative bit for bit).
+  template <int KIND>
+  __device__ __forceinline__ void md_job(int w0, int S, int cw0, int cs, bool own, int j0, int j1, int SK,
+                                         int ok) const {
+    using E = Expr<T>;
+    using F = Fp<T>;
+    T p = j0 > 0 ? win[w0 + 2 * (j0 - 1) * S] : T(0);
+    T a = win[w0 + 2 * j0 * S], b = win[w0 + 2 * (j0 + 1) * S];
+    T c = j0 + 2 <= 8 ? win[w0 + 2 * (j0 + 2) * S] : T(0);
+#pragma unroll 1
+    for (int j = j0; j < j1; ++j) {
+      const int wi = w0 + (2 * j + 1) * S;
+      const int oj = j == 0 ? 2 : (j == 7 ? 3 : 4);
+      const T lj = oj == 4 ? E::cubic_lambda(p, a, b, c, nat) : (oj == 2 ? E::quad_r(a, b, c) : E::quad_l(p, a, b));
+      T pred = lj;
+      if (KIND == 1 && !(oj == 4 && ok != 4)) {
+        const T lk = line_md_rt(win + wi, SK, ok);
+        pred = (oj != 4 && ok == 4) ? lk : E::half(F::add(lj, lk));
+      }
+      emit_at(wi, cw0 + (2 * j + 1) * cs, own, pred);
+      p = a;
+      a = b;
+      b = c;
+      if (j + 3 <= 8) c = win[w0 + 2 * (j + 3) * S];
+    }
+  }
+  // md cube points (x odd, cy, cz) along x, cube_at's cases for interior
+  // orders with its summation order for three cubics
+  __device__ __forceinline__ void md_cube_job(int cy, int cz, int j0, int j1) const {
+    using E = Expr<T>;
+    using F = Fp<T>;
+    constexpr int SY = kWin, SZ = kWin * kWin;
+    const int w0 = (cz * kWin + cy) * kWin, cw0 = (cz * 16 + cy) * 16;
+    const int oy = order0(cy), oz = order0(cz);
+    T p = j0 > 0 ? win[w0 + 2 * (j0 - 1)] : T(0);
+    T a = win[w0 + 2 * j0], b = win[w0 + 2 * (j0 + 1)];
+    T c = j0 + 2 <= 8 ? win[w0 + 2 * (j0 + 2)] : T(0);
+#pragma unroll 1
+    for (int j = j0; j < j1; ++j) {
+      const int wi = w0 + 2 * j + 1;
+      const T* w = win + wi;
+      const int ox = j == 0 ? 2 : (j == 7 ? 3 : 4);
+      T pred;
+      if (ox == 4) {
+        const T cx = E::cubic_lambda(p, a, b, c, nat);
+        if (oz == 4 && oy == 4) {
+          const T cy_ = E::cubic_lambda(w[-3 * SY], w[-SY], w[SY], w[3 * SY], nat);
+          const T cz_ = E::cubic_lambda(w[-3 * SZ], w[-SZ], w[SZ], w[3 * SZ], nat);
+          pred = F::div(F::add(F::add(cx, cy_), cz_), T(3));
+        } else if (oz == 4) {
+          pred = E::half(F::add(E::cubic_lambda(w[-3 * SZ], w[-SZ], w[SZ], w[3 * SZ], nat), cx));
+        } else if (oy == 4) {
+          pred = E::half(F::add(E::cubic_lambda(w[-3 * SY], w[-SY], w[SY], w[3 * SY], nat), cx));
+        } else {
+          pred = cx;
+        }
+      } else if (oz == 4 || oy == 4) {
+        if (oz == 4 && oy == 4)
+          pred = E::half(F::add(E::cubic_lambda(w[-3 * SZ], w[-SZ], w[SZ], w[3 * SZ], nat),
+                                E::cubic_lambda(w[-3 * SY], w[-SY], w[SY], w[3 * SY], nat)));
+        else if (oz == 4)
+          pred = E::cubic_lambda(w[-3 * SZ], w[-SZ], w[SZ], w[3 * SZ], nat);
+        else
+          pred = E::cubic_lambda(w[-3 * SY], w[-SY], w[SY], w[3 * SY], nat);
+      } else if (ox == 3) {
+        pred = E::quad_l(p, a, b);
+      } else {
+        pred = E::quad_r_cube(a, b, c);
+      }
+      emit_at(wi, cw0 + 2 * j + 1, true, pred);
+      p = a;
+      a = b;
+      b = c;
+      if (j + 3 <= 8) c = win[w0 + 2 * (j + 3)];
+    }
+  }
+  // md level 0: lines (243 jobs), faces (216 jobs), cube (256 quarter-line
+  // jobs), one barrier per stage
+  __device__ __forceinline__ void level0_md_lines() const {
+    static_assert(kPredThreads == 256, "one cube quarter-line per thread");
+    const int t = threadIdx.x;
+    auto kS = [](int a) { return a == 0 ? 1 : (a == 1 ? kWin : kWin * kWin); };  // window stride
+    auto kC = [](int a) { return a == 0 ? 1 : (a == 1 ? 16 : 256); };          // code-block stride
+    if (t < 243) {
+      // family f: lines along axis f through the other two (even) coordinates
+      const int f = t / 81, l = t - 81 * f, u = 2 * (l % 9), v = 2 * (l / 9);
+      const int P = f == 0 ? 1 : 0, Q = f == 2 ? 1 : 2;  // the fixed axes
+      const int w0 = u * kS(P) + v * kS(Q);
+      md_job<0>(w0, kS(f), u * kC(P) + v * kC(Q), kC(f), (u | v) < 16, 0, 8, 0, 0);
+    }
+    __syncthreads();
+    if (t < 216) {
+      // family f: the even axis EA = f; jobs along J, second odd axis K
+      const int f = t / 72, l = t - 72 * f, ce = 2 * (l % 9), ck = 2 * (l / 9) + 1;
+      const int J = f == 0 ? 1 : 0, K = f == 1 ? 2 : (f == 0 ? 2 : 1);
+      const int w0 = ce * kS(f) + ck * kS(K);
+      md_job<1>(w0, kS(J), ce * kC(f) + ck * kC(K), kC(J), ce < 16, 0, 8, kS(K), order0(ck));
+    }
+    __syncthreads();
+    {
+      const int line = t >> 2, q = t & 3;
+      md_cube_job(2 * (line & 7) + 1, 2 * (line >> 3) + 1, 2 * q, 2 * q + 2);
+    }
+    __syncthreads();
+  }
+  // The three stages by lines.  Points that no later prediction reads and
+  // whose codes belong to a neighbouring tile (the last stage's lines at
+  // coordinate 16, the middle stage's lines in the last stage's plane 16)
+  // are skipped: their values and codes would be dropped.  First stage: 81
+  // lines as 162 half-line jobs; middle stage: 144 lines; last stage: the
+  // tile's 256 lines, one per thread.
+  __device__ __forceinline__ void level0_lines(bool rev) const {
+    static_assert(kPredThreads == 256, "one last-stage line per thread");
+    const int t = threadIdx.x;
+    if (!rev) {  // z, then y, then x
+      if (t < 162) {
+        const int l = t >> 1, x = 2 * (l % 9), y = 2 * (l / 9);
+        if (t & 1) line_job<2, 4, 8>(x, y);
+        else line_job<2, 0, 4>(x, y);
+      }
+      __syncthreads();
+      if (t < 144) {
+        line_job<1, 0, 4>(2 * (t % 9), t / 9);
+        line_job<1, 4, 8>(2 * (t % 9), t / 9);
+      }
+      __syncthreads();
+      line_job<0, 0, 4>(t & 15, t >> 4);
+      line_job<0, 4, 8>(t & 15, t >> 4);
+    } else {  // x, then y, then z
+      if (t < 162) {
+        const int l = t >> 1, y = 2 * (l % 9), z = 2 * (l / 9);
+        if (t & 1) line_job<0, 4, 8>(y, z);
+        else line_job<0, 0, 4>(y, z);
+      }
+      __syncthreads();
+      if (t < 144) {
+        line_job<1, 0, 4>(t & 15, 2 * (t >> 4));
+        line_job<1, 4, 8>(t & 15, 2 * (t >> 4));
+      }
+      __syncthreads();
+      line_job<2, 0, 4>(t & 15, t >> 4);
+      line_job<2, 4, 8>(t & 15, t >> 4);
+    }
+    __syncthreads();
+  }
   // the three stages of the level (spline_layout_interpolate :1771-2027)
   __device__ __forceinline__ void run(bool md, bool rev) const {
     constexpr bool kLast = U == 1;
     // axis codes: x = 0, y = 1, z = 2; AXES = a0 | a1 << 2 | a2 << 4
+    if constexpr (!EDGE && U == 1) {
+      if (md) level0_md_lines();
+      else level0_lines(rev);
+      return;
+    }
     if (md) {
       // lines (xyzmap_line): x-lines vary y fastest, y- and z-lines vary x.
       // Points of one stage only read coarser points, so the three groups

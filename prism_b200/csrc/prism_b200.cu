@@ -100,8 +100,10 @@ struct prism_handle {
   int sm_count = 148;
   uint64_t launches = 0;       // kernels launched by this handle
   bool prof = false;
-  cudaEvent_t ev[kStCount][2] = {};
-  bool pending[kStCount] = {};
+  // per stage, one event pair per launch since the last collection (steps
+  // are enqueued back to back, so several launches of a stage can be pending)
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[kStCount];
+  int ev_used[kStCount] = {};
   double acc_ms[kStCount] = {};
   int acc_n[kStCount] = {};
   // side stream for the edge-tile launches, which run beside the interior
@@ -157,24 +159,36 @@ static cudaError_t fork_join(prism_handle* h, cudaStream_t st, bool have_interio
 }
 
 static void prof_begin(prism_handle* h, int stage, cudaStream_t st) {
-  if (h->prof) cudaEventRecord(h->ev[stage][0], st);
+  if (!h->prof) return;
+  auto& v = h->ev[stage];
+  if (h->ev_used[stage] == (int)v.size()) {
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (cudaEventCreate(&a) != cudaSuccess) return;
+    if (cudaEventCreate(&b) != cudaSuccess) {
+      cudaEventDestroy(a);
+      return;
+    }
+    v.emplace_back(a, b);
+  }
+  cudaEventRecord(v[h->ev_used[stage]].first, st);
+  h->ev_used[stage] += 1;
 }
 static void prof_end(prism_handle* h, int stage, cudaStream_t st) {
-  if (h->prof) {
-    cudaEventRecord(h->ev[stage][1], st);
-    h->pending[stage] = true;
-  }
+  if (!h->prof || h->ev_used[stage] == 0) return;
+  cudaEventRecord(h->ev[stage][h->ev_used[stage] - 1].second, st);
 }
-// after a stream sync: fold the recorded stage times into the accumulators
+// fold the recorded stage times into the accumulators (waits for them)
 static void prof_collect(prism_handle* h) {
   for (int i = 0; i < kStCount; ++i) {
-    if (!h->pending[i]) continue;
-    float ms = 0;
-    if (cudaEventElapsedTime(&ms, h->ev[i][0], h->ev[i][1]) == cudaSuccess) {
-      h->acc_ms[i] += ms;
-      h->acc_n[i] += 1;
+    for (int k = 0; k < h->ev_used[i]; ++k) {
+      float ms = 0;
+      const auto& e = h->ev[i][k];
+      if (cudaEventSynchronize(e.second) == cudaSuccess && cudaEventElapsedTime(&ms, e.first, e.second) == cudaSuccess) {
+        h->acc_ms[i] += ms;
+        h->acc_n[i] += 1;
+      }
     }
-    h->pending[i] = false;
+    h->ev_used[i] = 0;
   }
 }
 
@@ -621,8 +635,10 @@ void prism_destroy(prism_handle* h) {
                     &h->anchors, &h->small, &h->dev_in, &h->dev_out, &h->zero_anchors, &h->prog_slots};
   for (DevBuf* b : bufs) b->release();
   for (int i = 0; i < kStCount; ++i)
-    for (int j = 0; j < 2; ++j)
-      if (h->ev[i][j]) cudaEventDestroy(h->ev[i][j]);
+    for (auto& e : h->ev[i]) {
+      cudaEventDestroy(e.first);
+      cudaEventDestroy(e.second);
+    }
   if (h->side) cudaStreamDestroy(h->side);
   if (h->fork) cudaEventDestroy(h->fork);
   if (h->join) cudaEventDestroy(h->join);
@@ -635,17 +651,13 @@ const char* prism_last_error(const prism_handle* h) { return h ? h->err.c_str() 
 
 int prism_profile(prism_handle* h, int enable) {
   if (!h) return PRISM_ERR_ARG;
-  if (enable && !h->ev[0][0]) {
-    for (int i = 0; i < kStCount; ++i)
-      for (int j = 0; j < 2; ++j)
-        if (cudaEventCreate(&h->ev[i][j]) != cudaSuccess) return fail(h, PRISM_ERR_CUDA, "cudaEventCreate");
-  }
   h->prof = enable != 0;
   return PRISM_OK;
 }
 
 int prism_stage_times(prism_handle* h, double* ms, int* counts, int n, int reset) {
   if (!h || !ms) return PRISM_ERR_ARG;
+  prof_collect(h);
   for (int i = 0; i < n && i < kStCount; ++i) {
     ms[i] = h->acc_ms[i];
     if (counts) counts[i] = h->acc_n[i];
