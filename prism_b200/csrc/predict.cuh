@@ -454,39 +454,6 @@ struct LevelSweep {
   // quadratic from the left, cubic in between.
   // order along an axis at odd coordinate c of an interior tile, level 0
   static __device__ __forceinline__ int order0(int c) { return c == 1 ? 2 : (c == 15 ? 3 : 4); }
-  // line_at at point 2j+1 of a job, from the job's even values e[k] (at 2k)
-  template <bool MD>
-  __device__ __forceinline__ T job_line(const T (&e)[9], int j) const {
-    using E = Expr<T>;
-    if (j == 0) return E::quad_r(e[0], e[1], e[2]);
-    if (j == 7) return E::quad_l(e[6], e[7], e[8]);
-    return MD ? E::cubic_lambda(e[j - 1], e[j], e[j + 1], e[j + 2], nat)
-              : E::cubic_axis(e[j - 1], e[j], e[j + 1], e[j + 2], nat);
-  }
-  // the even values a job of points [J0, J1) reads along its axis
-  template <int S, int J0, int J1>
-  __device__ __forceinline__ void job_evens(int w0, T (&e)[9]) const {
-    constexpr int K0 = J0 > 0 ? J0 - 1 : 0, K1 = J1 + 2 < 9 ? J1 + 2 : 9;
-#pragma unroll
-    for (int k = K0; k < K1; ++k) e[k] = win[w0 + 2 * k * S];
-  }
-  template <int AX, int J0, int J1, bool MD = false>
-  __device__ __forceinline__ void line_job(int p, int q) const {
-    constexpr int S = kStride[AX];
-    constexpr int P = AX == 0 ? 1 : 0, Q = AX == 2 ? 1 : 2;
-    int c[3];
-    c[P] = p;
-    c[Q] = q;
-    c[AX] = 0;
-    const int w0 = (c[2] * kWin + c[1]) * kWin + c[0];
-    T e[9];
-    job_evens<S, J0, J1>(w0, e);
-#pragma unroll
-    for (int j = J0; j < J1; ++j) {
-      c[AX] = 2 * j + 1;
-      emit(w0 + (2 * j + 1) * S, c, job_line<MD>(e, j));
-    }
-  }
   // ---- md level 0 of an interior tile by jobs along one odd axis ----------
   // A job walks the odd points 2j+1, j in [j0, j1), of a line with window
   // stride S, holding the line's even values E[j-1..j+2] in a sliding window
@@ -512,6 +479,7 @@ struct LevelSweep {
     return E::quad_r(t1, t2, w[3 * S]);
   }
   // KIND 0: md line points (prediction along the job axis only);
+  // KIND 2: per-axis points (the same with the per-axis cubic);
   // KIND 1: md faces, the job axis J and a second odd axis with stride SK
   // and order ok (face_at: both cubic -> the mean of the two lines, one cubic
   // -> that line, neither -> the mean; add() is commutative bit for bit).
@@ -527,7 +495,8 @@ struct LevelSweep {
     for (int j = j0; j < j1; ++j) {
       const int wi = w0 + (2 * j + 1) * S;
       const int oj = j == 0 ? 2 : (j == 7 ? 3 : 4);
-      const T lj = oj == 4 ? E::cubic_lambda(p, a, b, c, nat) : (oj == 2 ? E::quad_r(a, b, c) : E::quad_l(p, a, b));
+      const T lj = oj == 4 ? (KIND == 2 ? E::cubic_axis(p, a, b, c, nat) : E::cubic_lambda(p, a, b, c, nat))
+                           : (oj == 2 ? E::quad_r(a, b, c) : E::quad_l(p, a, b));
       T pred = lj;
       if (KIND == 1 && !(oj == 4 && ok != 4)) {
         const T lk = line_md_rt(win + wi, SK, ok);
@@ -619,43 +588,42 @@ struct LevelSweep {
     }
     __syncthreads();
   }
-  // The three stages by lines.  Points that no later prediction reads and
-  // whose codes belong to a neighbouring tile (the last stage's lines at
-  // coordinate 16, the middle stage's lines in the last stage's plane 16)
-  // are skipped: their values and codes would be dropped.  First stage: 81
-  // lines as 162 half-line jobs; middle stage: 144 lines; last stage: the
-  // tile's 256 lines, one per thread.
+  // Per-axis level 0 of an interior tile by jobs (md_job<2>).  Points that no
+  // later prediction reads and whose codes belong to a neighbouring tile
+  // (the last stage's lines at coordinate 16, the middle stage's lines in
+  // the last stage's plane 16) are skipped: their values and codes would be
+  // dropped.  First stage: 81 lines as 162 half-line jobs; middle stage: 144
+  // lines; last stage: the tile's 256 lines, one per thread.
   __device__ __forceinline__ void level0_lines(bool rev) const {
     static_assert(kPredThreads == 256, "one last-stage line per thread");
+    constexpr int SY = kWin, SZ = kWin * kWin;
     const int t = threadIdx.x;
     if (!rev) {  // z, then y, then x
       if (t < 162) {
-        const int l = t >> 1, x = 2 * (l % 9), y = 2 * (l / 9);
-        if (t & 1) line_job<2, 4, 8>(x, y);
-        else line_job<2, 0, 4>(x, y);
+        const int l = t >> 1, x = 2 * (l % 9), y = 2 * (l / 9), j0 = (t & 1) * 4;
+        md_job<2>(x + y * SY, SZ, x + 16 * y, 256, (x | y) < 16, j0, j0 + 4, 0, 0);
       }
       __syncthreads();
       if (t < 144) {
-        line_job<1, 0, 4>(2 * (t % 9), t / 9);
-        line_job<1, 4, 8>(2 * (t % 9), t / 9);
+        const int x = 2 * (t % 9), z = t / 9;
+        md_job<2>(x + z * SZ, SY, x + 256 * z, 16, x < 16, 0, 8, 0, 0);
       }
       __syncthreads();
-      line_job<0, 0, 4>(t & 15, t >> 4);
-      line_job<0, 4, 8>(t & 15, t >> 4);
+      const int y = t & 15, z = t >> 4;
+      md_job<2>(y * SY + z * SZ, 1, 16 * y + 256 * z, 1, true, 0, 8, 0, 0);
     } else {  // x, then y, then z
       if (t < 162) {
-        const int l = t >> 1, y = 2 * (l % 9), z = 2 * (l / 9);
-        if (t & 1) line_job<0, 4, 8>(y, z);
-        else line_job<0, 0, 4>(y, z);
+        const int l = t >> 1, y = 2 * (l % 9), z = 2 * (l / 9), j0 = (t & 1) * 4;
+        md_job<2>(y * SY + z * SZ, 1, 16 * y + 256 * z, 1, (y | z) < 16, j0, j0 + 4, 0, 0);
       }
       __syncthreads();
       if (t < 144) {
-        line_job<1, 0, 4>(t & 15, 2 * (t >> 4));
-        line_job<1, 4, 8>(t & 15, 2 * (t >> 4));
+        const int x = t & 15, z = 2 * (t >> 4);
+        md_job<2>(x + z * SZ, SY, x + 256 * z, 16, z < 16, 0, 8, 0, 0);
       }
       __syncthreads();
-      line_job<2, 0, 4>(t & 15, t >> 4);
-      line_job<2, 4, 8>(t & 15, t >> 4);
+      const int x = t & 15, y = t >> 4;
+      md_job<2>(x + y * SY, SZ, x + 16 * y, 256, true, 0, 8, 0, 0);
     }
     __syncthreads();
   }
