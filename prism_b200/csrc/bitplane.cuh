@@ -8,12 +8,14 @@
 // a -> (a + 0xaaaaaaaa) ^ 0xaaaaaaaa).  Then bit 7-k of byte
 // planes[daprefix[l] + p*dstride[l] + g] is bit 31-p of w.
 //
-// B200 mapping: one warp handles 256 consecutive codes of one level.  Per 32
-// codes it loads one coalesced 128-byte row, does a 32x32 bit transpose with
-// five xor-shuffle rounds (lane i ends up holding bit i of all 32 codes, i.e.
-// plane 31-i), and after 8 rounds each lane stores the 32 bytes of its plane.
+// B200 mapping: one warp handles 1024 consecutive codes of one level; lane l
+// owns codes 32l..32l+31, i.e. the 4-byte word at byte 4l of every plane row
+// of the item.  The codes pass through a padded shared-memory tile (so that
+// global accesses stay coalesced 128-byte rows) and each lane turns its 32
+// codes into its 32 plane words with one in-register 32x32 bit transpose
+// (about 8 instructions per code instead of a shuffle network per code).
 // The inverse runs the same transpose backwards; the progressive inverse
-// zeroes the lanes of planes outside [begin, end) of each level.
+// leaves the words of planes outside [begin, end) of each level at zero.
 #pragma once
 #include "geometry.h"
 
@@ -21,18 +23,6 @@ namespace prism_b200 {
 
 constexpr int kShufWarps = 8;     // warps per CTA
 constexpr int kShufCodes = 1024;  // codes per warp work item (128 bytes per plane)
-
-__device__ __forceinline__ uint32_t warp_transpose32(uint32_t x, int lane) {
-  const uint32_t masks[5] = {0x0000FFFFu, 0x00FF00FFu, 0x0F0F0F0Fu, 0x33333333u, 0x55555555u};
-#pragma unroll
-  for (int s = 0; s < 5; ++s) {
-    int j = 16 >> s;
-    uint32_t m = masks[s];
-    uint32_t t = __shfl_xor_sync(0xffffffffu, x, j);
-    x = (lane & j) ? ((x & ~m) | ((t >> j) & m)) : ((x & m) | ((t & m) << j));
-  }
-  return x;
-}
 
 __device__ __forceinline__ uint32_t sign_transform(int32_t code, bool nb) {
   uint32_t a = (uint32_t)code;
@@ -45,9 +35,43 @@ __device__ __forceinline__ int32_t sign_inverse(uint32_t a, bool nb) {
   return (int32_t)((a & 0x7fffffffu) ^ (uint32_t)((int32_t)a >> 31));
 }
 
-// plane word (bit k = code k of 32) <-> the 4 plane bytes in memory order
-__device__ __forceinline__ uint32_t to_plane_bytes(uint32_t w) { return __byte_perm(__brev(w), 0, 0x0123); }
-__device__ __forceinline__ uint32_t from_plane_bytes(uint32_t b) { return __brev(__byte_perm(b, 0, 0x0123)); }
+// In-register 32x32 bit transpose: afterwards a[i] bit b = (before) a[b] bit i.
+// Recursive block swap over rounds j = 16, 8, 4, 2, 1: rows r and r + j
+// exchange their off-diagonal j-bit blocks (byte permutes for j = 16 and 8,
+// shift + select for the rest).
+template <int J>
+__device__ __forceinline__ void bit_swap_round(uint32_t (&a)[32], uint32_t m) {
+#pragma unroll
+  for (int r = 0; r < 32; ++r) {
+    if (r & J) continue;
+    const uint32_t x = a[r], y = a[r + J];
+    a[r] = (x & m) | ((y << J) & ~m);
+    a[r + J] = ((x >> J) & m) | (y & ~m);
+  }
+}
+__device__ __forceinline__ void bit_transpose32(uint32_t (&a)[32]) {
+#pragma unroll
+  for (int r = 0; r < 16; ++r) {
+    const uint32_t x = a[r], y = a[r + 16];
+    a[r] = __byte_perm(x, y, 0x5410);
+    a[r + 16] = __byte_perm(x, y, 0x7632);
+  }
+#pragma unroll
+  for (int r = 0; r < 32; ++r) {
+    if (r & 8) continue;
+    const uint32_t x = a[r], y = a[r + 8];
+    a[r] = __byte_perm(x, y, 0x6240);
+    a[r + 8] = __byte_perm(x, y, 0x7351);
+  }
+  bit_swap_round<4>(a, 0x0F0F0F0Fu);
+  bit_swap_round<2>(a, 0x33333333u);
+  bit_swap_round<1>(a, 0x55555555u);
+}
+// Bit k of a plane word as loaded (little-endian) belongs to code
+// sigma(k) = 8 (k / 8) + 7 - k % 8 of the word's 32 codes (bytes in memory
+// order, most significant bit first).
+__device__ __forceinline__ constexpr int plane_bit_code(int k) { return 8 * (k >> 3) + 7 - (k & 7); }
+
 
 // a[i] of a 4-entry array held in kernel parameters, without the local-memory
 // copy a dynamic index would force
@@ -91,9 +115,11 @@ __device__ __forceinline__ void locate_item(const ShufPlan& s, int64_t item, int
 }
 
 // codes (qc + anchors, device code space) -> planes.  A warp takes 1024
-// consecutive codes of one level: 32 coalesced 128-byte loads, 32 register
-// transposes, then through a padded shared-memory tile so that each plane's
-// 128 bytes leave as one contiguous warp store.
+// consecutive codes of one level: 32 coalesced 128-byte loads into a padded
+// shared-memory tile, from which lane l takes its 32 consecutive codes
+// 32l..32l+31 (in plane-bit order), one in-register 32x32 bit transpose, and
+// each plane's word of lane l is its 4 bytes of the plane row: one
+// contiguous 128-byte warp store per plane.
 // One warp work item of the forward shuffle (tw: the warp's staging tile).
 __device__ __forceinline__ void shuffle_item(uint32_t (&tw)[32][33], const int32_t* __restrict__ codes,
                                              uint8_t* __restrict__ planes, const Geometry& g, const ShufPlan& plan,
@@ -106,29 +132,32 @@ __device__ __forceinline__ void shuffle_item(uint32_t (&tw)[32][33], const int32
   int64_t count = pick4(plan.proc, level) - first;
   if (count > kShufCodes) count = kShufCodes;
   const int32_t* src = codes + pick4(plan.seg_start, level) + first;
-  if (count == kShufCodes) {
+  // tw[it][j] = transformed code 32 it + j (0 past the end: sign_transform(0)
+  // = 0); all 32 loads are issued before the first store
+  {
     int32_t c[32];
 #pragma unroll
-    for (int it = 0; it < 32; ++it) c[it] = __ldg(src + it * 32 + lane);
-#pragma unroll
-    for (int it = 0; it < 32; ++it) tw[lane][it] = to_plane_bytes(warp_transpose32(sign_transform(c[it], nb), lane));
-  } else {
-#pragma unroll 4
     for (int it = 0; it < 32; ++it) {
-      int idx = it * 32 + lane;
-      int32_t c = idx < count ? __ldg(src + idx) : 0;
-      tw[lane][it] = to_plane_bytes(warp_transpose32(sign_transform(c, nb), lane));
+      const int idx = it * 32 + lane;
+      c[it] = idx < count ? __ldg(src + idx) : 0;
     }
+#pragma unroll
+    for (int it = 0; it < 32; ++it) tw[it][lane] = sign_transform(c[it], nb);
   }
   __syncwarp();
-  // row r holds plane 31 - r; word j = plane bytes 4j..4j+3 of this item
+  uint32_t a[32];
+#pragma unroll
+  for (int k = 0; k < 32; ++k) a[k] = tw[lane][plane_bit_code(k)];
+  __syncwarp();  // the tile is free for the warp's next item
+  bit_transpose32(a);
+  // a[r] = the lane's word of plane 31 - r
   const int nbytes = (int)(count / 8);
   const int64_t stride = pick4(g.dstride, level);
   uint8_t* base = planes + pick4(g.daprefix, level) + first / 8;
-#pragma unroll 4
+#pragma unroll
   for (int r = 0; r < 32; ++r) {
     uint8_t* dst = base + (int64_t)(31 - r) * stride;
-    uint32_t w = tw[r][lane];
+    const uint32_t w = a[r];
     if (4 * lane + 4 <= nbytes) {
       reinterpret_cast<uint32_t*>(dst)[lane] = w;
     } else if (4 * lane < nbytes) {
@@ -168,29 +197,33 @@ inverse_bitshuffle_kernel(const uint8_t* __restrict__ planes, int32_t* __restric
   const int64_t stride = pick4(g.dstride, level);
   const uint8_t* base = planes + pick4(g.daprefix, level) + first / 8;
   uint32_t (&tw)[32][33] = tile[warp];
-  uint32_t v[32];
+  // a[r] = the lane's word (as loaded) of plane 31 - r
+  uint32_t a[32];
 #pragma unroll
   for (int r = 0; r < 32; ++r) {
     const int p = 31 - r;
     const uint8_t* src = base + (int64_t)p * stride;
-    v[r] = 0;
+    uint32_t v = 0;
     if (p >= lo && p < hi) {
       if (4 * lane + 4 <= nbytes) {
-        v[r] = __ldg(reinterpret_cast<const uint32_t*>(src) + lane);
+        v = __ldg(reinterpret_cast<const uint32_t*>(src) + lane);
       } else if (4 * lane < nbytes) {
-        for (int b = 4 * lane; b < nbytes; ++b) v[r] |= (uint32_t)src[b] << (8 * (b & 3));
+        for (int b = 4 * lane; b < nbytes; ++b) v |= (uint32_t)src[b] << (8 * (b & 3));
       }
     }
+    a[r] = v;
   }
+  bit_transpose32(a);
+  // a[k] = transformed code 32 lane + plane_bit_code(k); out through the tile
+  // so that the codes leave in coalesced rows
 #pragma unroll
-  for (int r = 0; r < 32; ++r) tw[r][lane] = v[r];
+  for (int k = 0; k < 32; ++k) tw[lane][plane_bit_code(k)] = a[k];
   __syncwarp();
   int32_t* dst = codes + pick4(plan.seg_start, level) + first;
-#pragma unroll 4
+#pragma unroll 8
   for (int it = 0; it < 32; ++it) {
-    uint32_t w = warp_transpose32(from_plane_bytes(tw[lane][it]), lane);
-    int idx = it * 32 + lane;
-    if (idx < count) dst[idx] = sign_inverse(w, nb);
+    const int idx = it * 32 + lane;
+    if (idx < count) dst[idx] = sign_inverse(tw[it][lane], nb);
   }
 }
 
