@@ -116,6 +116,10 @@ struct prism_handle {
   uint64_t prog_used = 0;
   ProgMirror* prog_host = nullptr;  // 64 mapped mirrors, one per slot
   ProgMirror* prog_host_dev = nullptr;
+  // per slot: the chunk offsets of the slot's container, computed by its
+  // first step and reused by the later ones
+  DevBuf prog_offs[64];
+  size_t zero_anchors_ready = 0;  // leading bytes of zero_anchors known to be zero
 };
 
 constexpr int kProgSlotBytes = 128;  // StrategyState + error flag
@@ -208,6 +212,7 @@ struct prism_prog {
   StrategyState* d_state = nullptr;
   int* d_err = nullptr;         // chunk errors of every step so far
   int slot = -1;                // slot in the handle's state block, or -1 (own allocation)
+  bool offs_ready = false;      // the slot's chunk offsets hold this container's
   ProgMirror* mirror = nullptr;      // mapped host copy written by each step
   ProgMirror* mirror_dev = nullptr;
   uint64_t loaded = 0;          // host copy, valid when !pending
@@ -476,15 +481,28 @@ static int launch_encode(prism_handle* h, const uint8_t* planes, const Geometry&
 }
 
 // err: where chunk errors go; null = the handle's flag, reset here
-static int launch_decode(prism_handle* h, const uint8_t* stream, uint64_t stream_bytes, const Geometry& g,
-                         const int* dbegin, const int* dend, uint8_t* planes, cudaStream_t st, int* err = nullptr) {
-  Small* s = small(h);
+// payload offset of every chunk: exclusive prefix sum of the size table
+static void launch_chunk_offsets(prism_handle* h, const uint8_t* stream, const Geometry& g, int64_t* offs,
+                                 cudaStream_t st) {
   const uint16_t* sizes = reinterpret_cast<const uint16_t*>(stream + 8);
   int64_t nblk = (g.chunks + kScanItems - 1) / kScanItems;
-  prof_begin(h, kStDecode, st);
-  scan_sizes_block<<<(unsigned)nblk, 1024, 0, st>>>(sizes, g.chunks, h->offs.as<int64_t>(), h->bsum.as<int64_t>());
+  scan_sizes_block<<<(unsigned)nblk, 1024, 0, st>>>(sizes, g.chunks, offs, h->bsum.as<int64_t>());
   scan_block_sums<<<1, 32, 0, st>>>(h->bsum.as<int64_t>(), nblk);
-  scan_add<<<(unsigned)((g.chunks + 255) / 256), 256, 0, st>>>(h->offs.as<int64_t>(), g.chunks, h->bsum.as<int64_t>());
+  scan_add<<<(unsigned)((g.chunks + 255) / 256), 256, 0, st>>>(offs, g.chunks, h->bsum.as<int64_t>());
+  h->launches += 3;
+}
+
+// offs_in: chunk offsets already computed for this stream (else computed here)
+static int launch_decode(prism_handle* h, const uint8_t* stream, uint64_t stream_bytes, const Geometry& g,
+                         const int* dbegin, const int* dend, uint8_t* planes, cudaStream_t st, int* err = nullptr,
+                         const int64_t* offs_in = nullptr) {
+  Small* s = small(h);
+  prof_begin(h, kStDecode, st);
+  const int64_t* offs = offs_in;
+  if (!offs) {
+    launch_chunk_offsets(h, stream, g, h->offs.as<int64_t>(), st);
+    offs = h->offs.as<int64_t>();
+  }
   if (!err) {
     err = &s->error_flag;
     CK(cudaMemsetAsync(err, 0, sizeof(int), st));
@@ -496,10 +514,9 @@ static int launch_decode(prism_handle* h, const uint8_t* stream, uint64_t stream
     attr_set = true;
   }
   int blocks = (int)std::min<int64_t>(g.chunks, (int64_t)h->sm_count * 8);
-  zbpc_decode_kernel<<<blocks, kZThreads, smem, st>>>(stream, stream_bytes, h->offs.as<int64_t>(), g, planes,
-                                                      dbegin, dend, err);
+  zbpc_decode_kernel<<<blocks, kZThreads, smem, st>>>(stream, stream_bytes, offs, g, planes, dbegin, dend, err);
   prof_end(h, kStDecode, st);
-  h->launches += 4;
+  h->launches += 1;
   CK(cudaGetLastError());
   return PRISM_OK;
 }
@@ -593,6 +610,8 @@ static int decompress_t(prism_handle* h, const uint8_t* cont, uint64_t size, con
   if (rc) return rc;
   if (size < g.header_size + 8 + 2 * (uint64_t)g.chunks) return fail(h, PRISM_ERR_CORRUPT, "container too small");
   const uint8_t* tr = cont + (size - g.header_size);
+  if (reinterpret_cast<uintptr_t>(tr) % sizeof(T))  // the anchors are read in place
+    return fail(h, PRISM_ERR_ARG, "container trailer not aligned to the value type");
   Small* s = small(h);
   CK(cudaMemcpyAsync(&s->range, tr + 8, sizeof(double), cudaMemcpyDeviceToDevice, st));
   params_kernel<T><<<1, 32, 0, st>>>(mode, bound, &s->range, alpha_of(mode == 1 ? bound : 0.0), nullptr, 0, tr, 4,
@@ -634,6 +653,7 @@ void prism_destroy(prism_handle* h) {
   DevBuf* bufs[] = {&h->qc, &h->planes, &h->status, &h->offs, &h->bsum, &h->part, &h->wins, &h->ranges,
                     &h->anchors, &h->small, &h->dev_in, &h->dev_out, &h->zero_anchors, &h->prog_slots};
   for (DevBuf* b : bufs) b->release();
+  for (DevBuf& b : h->prog_offs) b.release();
   for (int i = 0; i < kStCount; ++i)
     for (auto& e : h->ev[i]) {
       cudaEventDestroy(e.first);
@@ -776,6 +796,10 @@ int prism_progressive_open(prism_handle* h, const void* d_container, uint64_t si
     delete p;
     return fail(h, PRISM_ERR_CORRUPT, "container too small");
   }
+  if ((reinterpret_cast<uintptr_t>(d_container) | (size - p->g.header_size)) & 7) {
+    delete p;  // the trailer's doubles and 64-bit sizes are read in place
+    return fail(h, PRISM_ERR_ARG, "container or its trailer not 8-byte aligned");
+  }
   p->mode = mode;
   p->bound = bound;
   p->steps = 0;
@@ -811,6 +835,17 @@ int prism_progressive_open(prism_handle* h, const void* d_container, uint64_t si
   return PRISM_OK;
 }
 
+// strategy_finish_kernel + params_kernel of a progressive step in one launch
+template <class T>
+__global__ void prog_plan_kernel(const StrategyBlock* __restrict__ blk, int mode, double bound, double target,
+                                 const double* __restrict__ range, StrategyState* st, double alpha,
+                                 const uint8_t* __restrict__ flags, PredParams<T>* params, double* eb_out) {
+  strategy_finish_warp(blk, mode, bound, target, range, st);
+  if (threadIdx.x != 0) return;
+  compute_params<T>(mode, bound, range, alpha, nullptr, 0, flags, 4, params, nullptr, eb_out);
+  params->maxlevel = st->maxlevel;
+}
+
 __global__ void prog_init_kernel(StrategyState* st, int* err) {
   if (threadIdx.x < 4) { st->begin[threadIdx.x] = 0; st->end[threadIdx.x] = 0; }
   if (threadIdx.x == 0) { st->maxlevel = 4; *err = 0; }
@@ -840,11 +875,17 @@ static int progressive_step_t(prism_prog* p, double target, const T* prev, T* va
   const Geometry& g = p->g;
   int rc = ensure_common(h, g);
   if (rc) return rc;
-  CKA(h->zero_anchors.ensure(g.anchors * sizeof(T) + 64));
+  const size_t zbytes = g.anchors * sizeof(T) + 64;
+  if (h->zero_anchors.cap < zbytes) h->zero_anchors_ready = 0;
+  CKA(h->zero_anchors.ensure(zbytes));
+  if (h->zero_anchors_ready < zbytes) {  // the buffer is only ever read afterwards
+    CK(cudaMemsetAsync(h->zero_anchors.p, 0, h->zero_anchors.cap, st));
+    h->zero_anchors_ready = h->zero_anchors.cap;
+  }
   Small* s = small(h);
   const uint8_t* tr = p->cont + (p->size - g.header_size);
+  const double* range = reinterpret_cast<const double*>(tr + 8);
   bool first = p->steps == 0;
-  CK(cudaMemcpyAsync(&s->range, tr + 8, sizeof(double), cudaMemcpyDeviceToDevice, st));
   StrategyState* ds = p->d_state;
   if (first) {  // no planes loaded, all levels, no errors
     prog_init_kernel<<<1, 32, 0, st>>>(ds, p->d_err);
@@ -854,18 +895,27 @@ static int progressive_step_t(prism_prog* p, double target, const T* prev, T* va
   // it advances the object's device state in place
   const uint64_t* csbp = reinterpret_cast<const uint64_t*>(tr + 16);
   prof_begin(h, kStStrategy, st);
-  strategy_search_kernel<<<33, 1024, 0, st>>>(csbp, p->mode, p->bound, target, &s->range, s->sblk);
-  strategy_finish_kernel<<<1, 32, 0, st>>>(s->sblk, p->mode, p->bound, target, &s->range, ds);
+  strategy_search_kernel<<<33, 1024, 0, st>>>(csbp, p->mode, p->bound, target, range, s->sblk);
+  // the strategy's plane ranges, then the parameters with its maxlevel
+  prog_plan_kernel<T><<<1, 32, 0, st>>>(s->sblk, p->mode, p->bound, target, range, ds,
+                                        alpha_of(p->mode == 1 ? p->bound : 0.0), tr,
+                                        reinterpret_cast<PredParams<T>*>(s->params), &s->eb);
   prof_end(h, kStStrategy, st);
-  h->launches += 3;
-  // parameters with maxlevel from the strategy
-  params_kernel<T><<<1, 32, 0, st>>>(p->mode, p->bound, &s->range, alpha_of(p->mode == 1 ? p->bound : 0.0), nullptr,
-                                     0, tr, 4, reinterpret_cast<PredParams<T>*>(s->params), nullptr, &s->eb);
-  CK(cudaMemcpyAsync(&reinterpret_cast<PredParams<T>*>(s->params)->maxlevel, &ds->maxlevel, sizeof(int),
-                     cudaMemcpyDeviceToDevice, st));
-  CK(cudaMemsetAsync(h->planes.p, 0, g.aligned_size, st));
+  h->launches += 2;
+  // chunk offsets: once per object when it holds a slot
+  const int64_t* offs = nullptr;
+  if (p->slot >= 0) {
+    DevBuf& ob = h->prog_offs[p->slot];
+    if (!p->offs_ready) {
+      CKA(ob.ensure(((size_t)g.chunks + 1) * sizeof(int64_t)));
+      launch_chunk_offsets(h, p->cont, g, ob.as<int64_t>(), st);
+      p->offs_ready = true;
+    }
+    offs = ob.as<int64_t>();
+  }
+  // chunks of planes the step does not load are written as zeros
   rc = launch_decode(h, p->cont, p->size - g.header_size, g, ds->begin, ds->end, h->planes.as<uint8_t>(), st,
-                     p->d_err);
+                     p->d_err, offs);
   if (rc) return rc;
   rc = launch_inverse(h, h->planes.as<uint8_t>(), g, 1 /*NB*/, ds->begin, ds->end, h->qc.as<int32_t>(), st);
   if (rc) return rc;
@@ -874,7 +924,6 @@ static int progressive_step_t(prism_prog* p, double target, const T* prev, T* va
     rc = launch_reconstruct<T, false>(h, h->qc.as<int32_t>(), reinterpret_cast<const T*>(tr + 1040), g,
                                       params_ptr<T>(h), nullptr, values, st);
   } else {
-    CK(cudaMemsetAsync(h->zero_anchors.p, 0, g.anchors * sizeof(T), st));
     rc = launch_reconstruct<T, true>(h, h->qc.as<int32_t>(), h->zero_anchors.as<T>(), g, params_ptr<T>(h), prev,
                                      values, st);
   }

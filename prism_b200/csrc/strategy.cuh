@@ -125,4 +125,45 @@ __global__ void strategy_finish_kernel(const StrategyBlock* __restrict__ blk, in
   *st = s;
 }
 
+// The same on one warp (lane 0 writes the state): the 33 block maxima reduce
+// by the same tree (at each stride, position t takes t + stride's entry when
+// its value is strictly smaller), so ties resolve identically.
+__device__ __forceinline__ void strategy_finish_warp(const StrategyBlock* __restrict__ blk, int mode, double bound,
+                                                     double target, const double* __restrict__ range,
+                                                     StrategyState* __restrict__ st) {
+  const int lane = threadIdx.x & 31;
+  bool use_search;
+  uint64_t target_cost;
+  strategy_setup(mode, bound, target, range, &use_search, &target_cost);
+  int winner = 0;
+  if (use_search) {
+    unsigned long long v = blk[lane].value;
+    int bid = lane;
+    const unsigned long long w32 = lane == 0 ? blk[32].value : 0ull;
+    if (v < w32) { v = w32; bid = 32; }
+    for (int stride = 16; stride > 0; stride >>= 1) {
+      const unsigned long long w = __shfl_down_sync(0xffffffffu, v, stride);
+      const int wb = __shfl_down_sync(0xffffffffu, bid, stride);
+      if (lane < stride && v < w) { v = w; bid = wb; }
+    }
+    winner = __shfl_sync(0xffffffffu, bid, 0);
+  }
+  if (lane != 0) return;
+  StrategyState s = *st;
+  int maxlevel = 4;
+  for (int i = 0; i < 4; ++i) s.begin[i] = s.end[i];
+  if (!use_search) {
+    for (int i = 0; i < 4; ++i) s.end[i] = 32;
+    maxlevel = s.begin[0] < 32 ? 3 : s.begin[1] < 32 ? 2 : s.begin[2] < 32 ? 1 : s.begin[3] < 32 ? 0 : 4;
+  } else {
+    const int* tg = blk[winner].target;
+    if (s.begin[3] < tg[3]) { s.end[3] = tg[3]; maxlevel = 0; } else s.end[3] = s.begin[3];
+    if (s.begin[2] < tg[2]) { s.end[2] = tg[2]; maxlevel = 1; } else s.end[2] = s.begin[2];
+    if (s.begin[1] < tg[1]) { s.end[1] = tg[1]; maxlevel = 2; } else s.end[1] = s.begin[1];
+    if (s.begin[0] < tg[0]) { s.end[0] = tg[0]; maxlevel = 3; } else s.end[0] = s.begin[0];
+  }
+  s.maxlevel = maxlevel;
+  *st = s;
+}
+
 }  // namespace prism_b200

@@ -459,7 +459,17 @@ zbpc_decode_kernel(const uint8_t* __restrict__ stream, uint64_t stream_bytes, co
     if (begin) {
       int64_t cpp = g.chunks_level[loc.level] >> 5;
       int64_t real = loc.plane * cpp + loc.offset;
-      if (real < begin[3 - loc.level] * cpp || real >= end[3 - loc.level] * cpp) continue;
+      if (real < begin[3 - loc.level] * cpp || real >= end[3 - loc.level] * cpp) {
+        // a plane this step does not load reads as zero (chunk sizes and
+        // offsets are multiples of 8, and the chunks tile the plane buffer)
+        const int b0 = tid * 32;
+        if (b0 < loc.osize) {
+          uint2* d2 = reinterpret_cast<uint2*>(planes + loc.base + b0);
+          const int nq = min(4, (loc.osize - b0) >> 3);
+          for (int q = 0; q < nq; ++q) d2[q] = make_uint2(0, 0);
+        }
+        continue;
+      }
     }
     const int osize = loc.osize;
     const int csize = sizes[id];
