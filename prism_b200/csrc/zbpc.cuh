@@ -424,17 +424,27 @@ struct DecodeShared {
   int flag;
 };
 
-// Copy n bytes from an arbitrarily aligned global address into shared memory
-// with aligned 32-bit loads; no byte past src + n - 1's word is read.
+// Copy n <= kChunk bytes from an arbitrarily aligned global address into
+// shared memory with aligned 32-bit loads; no byte past src + n - 1's word is
+// read.  A thread's words are w = t + k * kZThreads (k < 8); every load is
+// issued before the first store, so a chunk costs one load latency.
 __device__ __forceinline__ void copy_in(uint8_t* dst, const uint8_t* src, int n) {
+  constexpr int kWords = kChunk / 4 / kZThreads;
   const int shift = (int)((uintptr_t)src & 3);
   const uint32_t* a = reinterpret_cast<const uint32_t*>(src - shift);
   const int last = (shift + n - 1) >> 2;  // last source word needed
   uint32_t* dw = reinterpret_cast<uint32_t*>(dst);
-  for (int w = threadIdx.x; 4 * w < n; w += kZThreads) {
-    uint32_t lo = __ldg(a + w);
-    uint32_t hi = w + 1 <= last ? __ldg(a + w + 1) : 0u;
-    dw[w] = shift ? __funnelshift_r(lo, hi, 8 * shift) : lo;
+  uint32_t lo[kWords], hi[kWords];
+#pragma unroll
+  for (int k = 0; k < kWords; ++k) {
+    const int w = threadIdx.x + k * kZThreads;
+    lo[k] = 4 * w < n ? __ldg(a + w) : 0u;
+    hi[k] = (4 * w < n && w + 1 <= last) ? __ldg(a + w + 1) : 0u;
+  }
+#pragma unroll
+  for (int k = 0; k < kWords; ++k) {
+    const int w = threadIdx.x + k * kZThreads;
+    if (4 * w < n) dw[w] = shift ? __funnelshift_r(lo[k], hi[k], 8 * shift) : lo[k];
   }
 }
 
