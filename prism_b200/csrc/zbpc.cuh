@@ -37,15 +37,19 @@ struct ChunkLoc {
   bool last_of_plane;
 };
 
+// Chunk counts fit 32 bits (a plane buffer of 2^32 chunks would be 64 TB),
+// so the plane/offset split is a 32-bit division (a 64-bit one is a long
+// software sequence, run by every thread for every chunk).
 __host__ __device__ __forceinline__ ChunkLoc locate_chunk(const Geometry& g, int64_t id) {
   ChunkLoc c;
   int64_t real = id;
   int l = 3;
   while (l > 0 && real >= g.chunks_level[l]) real -= g.chunks_level[l--];
-  int64_t cpp = g.chunks_level[l] >> 5;
+  const uint32_t cpp = (uint32_t)(g.chunks_level[l] >> 5), r32 = (uint32_t)real;
+  const uint32_t plane = r32 / cpp;
   c.level = l;
-  c.plane = real / cpp;
-  c.offset = real % cpp;
+  c.plane = plane;
+  c.offset = r32 - plane * cpp;
   int64_t b = 0;
   for (int i = 3; i > l; --i) b += g.hastride[i] << 5;
   c.base = b + c.plane * g.hastride[l] + c.offset * kChunk;
