@@ -372,9 +372,16 @@ struct LevelSweep {
   T ebr, ebx2;
   bool nat;
 
-  // The reconstruction keeps each point's code, already converted with
-  // from_int, in the point's own window slot until the point is predicted
-  // (no prediction reads a point of its own or a later stage).
+  // The reconstruction keeps each point's code as an int32 in the low word of
+  // the point's own window slot until the point is predicted (no prediction
+  // reads a point of its own or a later stage), and converts it there.
+  __device__ __forceinline__ T code_of(int wi) const {
+    const T v = win[wi];  // read as T, then the low word: no type-punned access
+    int32_t c;
+    if constexpr (sizeof(T) == 8) c = __double2loint(v);
+    else c = __float_as_int(v);
+    return Fp<T>::from_int(c);
+  }
   // Compression keeps the codes of the tile's own 16^3 points only (the
   // codes of the shared faces belong to the neighbouring tiles).
   __device__ __forceinline__ void emit(int wi, const int c[3], T pred) const {
@@ -384,7 +391,7 @@ struct LevelSweep {
       if ((c[0] | c[1] | c[2]) < 16) cw[(c[2] * 16 + c[1]) * 16 + c[0]] = code;
       win[wi] = rec;
     } else {
-      win[wi] = Fp<T>::fma(win[wi], ebx2, pred);
+      win[wi] = Fp<T>::fma(code_of(wi), ebx2, pred);
     }
   }
   // xyz_predicate (:1173-1185)
@@ -467,7 +474,7 @@ struct LevelSweep {
       if (own) cw[cwi] = code;
       win[wi] = rec;
     } else {
-      win[wi] = Fp<T>::fma(win[wi], ebx2, pred);
+      win[wi] = Fp<T>::fma(code_of(wi), ebx2, pred);
     }
   }
   // line_at (MD) along a runtime stride with an interior order
@@ -894,8 +901,8 @@ reconstruct_kernel(const int32_t* __restrict__ qc, const T* __restrict__ anchors
     }
   }
   __syncthreads();
-  // each code lands in the low word of its window slot and is converted in
-  // place by the thread that copied it
+  // each code lands in the low word of its window slot (converted when its
+  // point is predicted); every other slot reads as zero
 #pragma unroll 4
   for (int i = tid; i < kWinVol; i += kPredThreads) {
     int x, y, z;
@@ -903,12 +910,9 @@ reconstruct_kernel(const int32_t* __restrict__ qc, const T* __restrict__ anchors
     const int lv = win_level(x, y, z);
     int32_t* dst = reinterpret_cast<int32_t*>(&sm.win[i]);
     if (lv < 4 && lv <= maxlevel && L.in_data(x, y, z)) copy_async<4>(dst, qc + slot_of(sm.rows, lv, x, y, z));
-    else *dst = 0;
+    else sm.win[i] = T(0);
   }
   copy_async_wait_all();
-#pragma unroll 4
-  for (int i = tid; i < kWinVol; i += kPredThreads)
-    sm.win[i] = Fp<T>::from_int(*reinterpret_cast<const int32_t*>(&sm.win[i]));
   __syncthreads();
   if (tid < 8) {  // x_reset_scratch_data (:1027-1067): anchors at the corners
     int x = (tid & 1) * 16, y = ((tid >> 1) & 1) * 16, z = (tid >> 2) * 16;
