@@ -566,6 +566,178 @@ struct LevelSweep {
       if (j + 3 <= 8) c = win[w0 + 2 * (j + 3)];
     }
   }
+  // ---- level 0 of an edge tile (the last slab along some axis) by jobs ----
+  // The same jobs as on interior tiles with the orders of order_of under the
+  // tile's runtime limits, and with jobs and points outside the field
+  // skipped (the generic sweeps skip them through pred_ok).
+  __device__ __forceinline__ int lim3(int d) const { return d == 0 ? L.l3(0) : (d == 1 ? L.l3(1) : L.l3(2)); }
+  __device__ __forceinline__ int lim1(int d) const { return d == 0 ? L.l1(0) : (d == 1 ? L.l1(1) : L.l1(2)); }
+  __device__ __forceinline__ int lim_r(int d) const { return d == 0 ? L.r(0) : (d == 1 ? L.r(1) : L.r(2)); }
+  static __device__ __forceinline__ int order_rt(int c, int l3, int l1) {
+    const bool f3 = c + 3 <= l3, f1 = c + 1 <= l1;
+    return c >= 3 ? (f3 ? 4 : (f1 ? 3 : 0)) : (f3 ? 2 : (f1 ? 1 : 0));
+  }
+  // line_at from a job's sliding window (p, a, b, c) = E[j-1..j+2]
+  template <bool MD>
+  __device__ __forceinline__ T window_line(int o, T p, T a, T b, T c) const {
+    using E = Expr<T>;
+    if (o == 4) return MD ? E::cubic_lambda(p, a, b, c, nat) : E::cubic_axis(p, a, b, c, nat);
+    if (o == 3) return E::quad_l(p, a, b);
+    if (o == 2) return E::quad_r(a, b, c);
+    if (o == 1) return E::lin(a, b);
+    return a;
+  }
+  // line_at (MD) along a runtime stride, every order
+  __device__ __forceinline__ T line_rt(const T* w, int S, int o) const {
+    using E = Expr<T>;
+    const T t1 = w[-S];
+    if (o == 0) return t1;
+    const T t2 = w[S];
+    if (o == 4) return E::cubic_lambda(w[-3 * S], t1, t2, w[3 * S], nat);
+    if (o == 3) return E::quad_l(w[-3 * S], t1, t2);
+    if (o == 2) return E::quad_r(t1, t2, w[3 * S]);
+    return E::lin(t1, t2);
+  }
+  // KIND 0 md lines, 2 per-axis lines, 1 md faces (J = the reference's a2,
+  // K = a1, at odd coordinate ck: face_at's full case table)
+  template <int KIND>
+  __device__ __forceinline__ void edge_job(int w0, int J, int K, int cw0, int cs, bool own, int j0, int j1,
+                                           int ck) const {
+    using E = Expr<T>;
+    using F = Fp<T>;
+    const int S = J == 0 ? 1 : (J == 1 ? kWin : kWin * kWin);
+    const int l3 = lim3(J), l1 = lim1(J), r = lim_r(J);
+    int SK = 0, ok = 0;
+    if (KIND == 1) {
+      SK = K == 0 ? 1 : (K == 1 ? kWin : kWin * kWin);
+      ok = order_rt(ck, lim3(K), lim1(K));
+    }
+    T p = j0 > 0 ? win[w0 + 2 * (j0 - 1) * S] : T(0);
+    T a = win[w0 + 2 * j0 * S], b = win[w0 + 2 * (j0 + 1) * S];
+    T c = j0 + 2 <= 8 ? win[w0 + 2 * (j0 + 2) * S] : T(0);
+#pragma unroll 1
+    for (int j = j0; j < j1 && 2 * j + 1 < r; ++j) {
+      const int wi = w0 + (2 * j + 1) * S;
+      const int oj = order_rt(2 * j + 1, l3, l1);
+      const T lj = window_line<KIND != 2>(oj, p, a, b, c);
+      T pred = lj;
+      if (KIND == 1) {
+        if (ok == 4 || oj == 4) {
+          if (ok != 4) pred = lj;
+          else if (oj != 4) pred = line_rt(win + wi, SK, ok);
+          else pred = E::half(F::add(line_rt(win + wi, SK, ok), lj));
+        } else if ((ok >= 2 && oj >= 2) || (ok == 1 && oj == 1)) {
+          pred = E::half(F::add(line_rt(win + wi, SK, ok), lj));
+        } else if (ok >= 2 || (ok == 1 && oj == 0)) {
+          pred = line_rt(win + wi, SK, ok);
+        } else if (oj >= 1) {
+          pred = lj;
+        } else {
+          pred = F::sub(F::add(win[wi - SK], win[wi - S]), win[wi - SK - S]);
+        }
+      }
+      emit_at(wi, cw0 + (2 * j + 1) * cs, own, pred);
+      p = a;
+      a = b;
+      b = c;
+      if (j + 3 <= 8) c = win[w0 + 2 * (j + 3) * S];
+    }
+  }
+  // md cube points (x odd, cy, cz) along x with cube_at's full case order
+  __device__ __forceinline__ void edge_cube_job(int cy, int cz, int j0, int j1) const {
+    using E = Expr<T>;
+    using F = Fp<T>;
+    constexpr int SY = kWin, SZ = kWin * kWin;
+    const int w0 = (cz * kWin + cy) * kWin, cw0 = (cz * 16 + cy) * 16;
+    const int oy = order_rt(cy, lim3(1), lim1(1)), oz = order_rt(cz, lim3(2), lim1(2));
+    const int l3 = lim3(0), l1 = lim1(0), r = lim_r(0);
+    T p = j0 > 0 ? win[w0 + 2 * (j0 - 1)] : T(0);
+    T a = win[w0 + 2 * j0], b = win[w0 + 2 * (j0 + 1)];
+    T c = j0 + 2 <= 8 ? win[w0 + 2 * (j0 + 2)] : T(0);
+#pragma unroll 1
+    for (int j = j0; j < j1 && 2 * j + 1 < r; ++j) {
+      const int wi = w0 + 2 * j + 1;
+      const T* w = win + wi;
+      const int ox = order_rt(2 * j + 1, l3, l1);
+      auto cy_ = [&]() { return E::cubic_lambda(w[-3 * SY], w[-SY], w[SY], w[3 * SY], nat); };
+      auto cz_ = [&]() { return E::cubic_lambda(w[-3 * SZ], w[-SZ], w[SZ], w[3 * SZ], nat); };
+      auto cx_ = [&]() { return E::cubic_lambda(p, a, b, c, nat); };
+      T pred;
+      if (oz == 4 && oy == 4 && ox == 4) pred = F::div(F::add(F::add(cx_(), cy_()), cz_()), T(3));
+      else if (oz == 4 && oy == 4) pred = E::half(F::add(cz_(), cy_()));
+      else if (oz == 4 && ox == 4) pred = E::half(F::add(cz_(), cx_()));
+      else if (oy == 4 && ox == 4) pred = E::half(F::add(cy_(), cx_()));
+      else if (oz == 4) pred = cz_();
+      else if (oy == 4) pred = cy_();
+      else if (ox == 4) pred = cx_();
+      else if (ox == 3) pred = E::quad_l(p, a, b);
+      else if (ox == 2) pred = E::quad_r_cube(a, b, c);
+      else if (ox == 1) pred = E::lin(a, b);
+      else pred = a;
+      emit_at(wi, cw0 + 2 * j + 1, true, pred);
+      p = a;
+      a = b;
+      b = c;
+      if (j + 3 <= 8) c = win[w0 + 2 * (j + 3)];
+    }
+  }
+  __device__ __forceinline__ void edge_md_lines() const {
+    const int t = threadIdx.x;
+    auto kS = [](int a) { return a == 0 ? 1 : (a == 1 ? kWin : kWin * kWin); };
+    auto kC = [](int a) { return a == 0 ? 1 : (a == 1 ? 16 : 256); };
+    if (t < 243) {
+      const int f = t / 81, l = t - 81 * f, u = 2 * (l % 9), v = 2 * (l / 9);
+      const int P = f == 0 ? 1 : 0, Q = f == 2 ? 1 : 2;
+      if (u < lim_r(P) && v < lim_r(Q))
+        edge_job<0>(u * kS(P) + v * kS(Q), f, 0, u * kC(P) + v * kC(Q), kC(f), (u | v) < 16, 0, 8, 0);
+    }
+    __syncthreads();
+    if (t < 216) {
+      const int f = t / 72, l = t - 72 * f, ce = 2 * (l % 9), ck = 2 * (l / 9) + 1;
+      const int J = f == 0 ? 1 : 0, K = f == 1 ? 2 : (f == 0 ? 2 : 1);
+      if (ce < lim_r(f) && ck < lim_r(K))
+        edge_job<1>(ce * kS(f) + ck * kS(K), J, K, ce * kC(f) + ck * kC(K), kC(J), ce < 16, 0, 8, ck);
+    }
+    __syncthreads();
+    {
+      const int line = t >> 2, q = t & 3, cy = 2 * (line & 7) + 1, cz = 2 * (line >> 3) + 1;
+      if (cy < lim_r(1) && cz < lim_r(2)) edge_cube_job(cy, cz, 2 * q, 2 * q + 2);
+    }
+    __syncthreads();
+  }
+  __device__ __forceinline__ void edge_axis_lines(bool rev) const {
+    constexpr int SY = kWin, SZ = kWin * kWin;
+    const int t = threadIdx.x;
+    const int r0 = lim_r(0), r1 = lim_r(1), r2 = lim_r(2);
+    if (!rev) {  // z, then y, then x
+      if (t < 162) {
+        const int l = t >> 1, x = 2 * (l % 9), y = 2 * (l / 9), j0 = (t & 1) * 4;
+        if (x < r0 && y < r1) edge_job<2>(x + y * SY, 2, 0, x + 16 * y, 256, (x | y) < 16, j0, j0 + 4, 0);
+      }
+      __syncthreads();
+      if (t < 144) {
+        const int x = 2 * (t % 9), z = t / 9;
+        if (x < r0 && z < r2) edge_job<2>(x + z * SZ, 1, 0, x + 256 * z, 16, x < 16, 0, 8, 0);
+      }
+      __syncthreads();
+      const int y = t & 15, z = t >> 4;
+      if (y < r1 && z < r2) edge_job<2>(y * SY + z * SZ, 0, 0, 16 * y + 256 * z, 1, true, 0, 8, 0);
+    } else {  // x, then y, then z
+      if (t < 162) {
+        const int l = t >> 1, y = 2 * (l % 9), z = 2 * (l / 9), j0 = (t & 1) * 4;
+        if (y < r1 && z < r2) edge_job<2>(y * SY + z * SZ, 0, 0, 16 * y + 256 * z, 1, (y | z) < 16, j0, j0 + 4, 0);
+      }
+      __syncthreads();
+      if (t < 144) {
+        const int x = t & 15, z = 2 * (t >> 4);
+        if (x < r0 && z < r2) edge_job<2>(x + z * SZ, 1, 0, x + 256 * z, 16, z < 16, 0, 8, 0);
+      }
+      __syncthreads();
+      const int x = t & 15, y = t >> 4;
+      if (x < r0 && y < r1) edge_job<2>(x + y * SY, 2, 0, x + 16 * y, 256, true, 0, 8, 0);
+    }
+    __syncthreads();
+  }
   // md level 0: lines (243 jobs), faces (216 jobs), cube (256 quarter-line
   // jobs), one barrier per stage
   __device__ __forceinline__ void level0_md_lines() const {
@@ -638,9 +810,14 @@ struct LevelSweep {
   __device__ __forceinline__ void run(bool md, bool rev) const {
     constexpr bool kLast = U == 1;
     // axis codes: x = 0, y = 1, z = 2; AXES = a0 | a1 << 2 | a2 << 4
-    if constexpr (!EDGE && U == 1) {
-      if (md) level0_md_lines();
-      else level0_lines(rev);
+    if constexpr (U == 1) {
+      if constexpr (EDGE) {
+        if (md) edge_md_lines();
+        else edge_axis_lines(rev);
+      } else {
+        if (md) level0_md_lines();
+        else level0_lines(rev);
+      }
       return;
     }
     if (md) {
