@@ -178,7 +178,7 @@ bitshuffle_kernel(const int32_t* __restrict__ codes, uint8_t* __restrict__ plane
 // planes -> codes; begin/end (device, may be null) restrict each level to
 // planes [begin[3-l], end[3-l]) exactly as the progressive inverse does.
 // Rows of planes outside that range are never read.
-__global__ void __launch_bounds__(kShufWarps * 32)
+__global__ void __launch_bounds__(kShufWarps * 32, 4)
 inverse_bitshuffle_kernel(const uint8_t* __restrict__ planes, int32_t* __restrict__ codes, Geometry g,
                           ShufPlan plan, int nb, const int* __restrict__ begin, const int* __restrict__ end) {
   __shared__ uint32_t tile[kShufWarps][32][33];
