@@ -573,9 +573,10 @@ struct LevelSweep {
   __device__ __forceinline__ int lim3(int d) const { return d == 0 ? L.l3(0) : (d == 1 ? L.l3(1) : L.l3(2)); }
   __device__ __forceinline__ int lim1(int d) const { return d == 0 ? L.l1(0) : (d == 1 ? L.l1(1) : L.l1(2)); }
   __device__ __forceinline__ int lim_r(int d) const { return d == 0 ? L.r(0) : (d == 1 ? L.r(1) : L.r(2)); }
+  // order_of at coordinate c (an odd multiple of the unit U)
   static __device__ __forceinline__ int order_rt(int c, int l3, int l1) {
-    const bool f3 = c + 3 <= l3, f1 = c + 1 <= l1;
-    return c >= 3 ? (f3 ? 4 : (f1 ? 3 : 0)) : (f3 ? 2 : (f1 ? 1 : 0));
+    const bool f3 = c + 3 * U <= l3, f1 = c + U <= l1;
+    return c >= 3 * U ? (f3 ? 4 : (f1 ? 3 : 0)) : (f3 ? 2 : (f1 ? 1 : 0));
   }
   // line_at from a job's sliding window (p, a, b, c) = E[j-1..j+2]
   template <bool MD>
@@ -599,26 +600,27 @@ struct LevelSweep {
     return E::lin(t1, t2);
   }
   // KIND 0 md lines, 2 per-axis lines, 1 md faces (J = the reference's a2,
-  // K = a1, at odd coordinate ck: face_at's full case table)
+  // K = a1, at odd coordinate ck: face_at's full case table).  Point j of a
+  // job is at coordinate (2j+1)U along J; its line's even values at 2kU.
   template <int KIND>
   __device__ __forceinline__ void edge_job(int w0, int J, int K, int cw0, int cs, bool own, int j0, int j1,
                                            int ck) const {
     using E = Expr<T>;
     using F = Fp<T>;
-    const int S = J == 0 ? 1 : (J == 1 ? kWin : kWin * kWin);
+    const int S = U * (J == 0 ? 1 : (J == 1 ? kWin : kWin * kWin));
     const int l3 = lim3(J), l1 = lim1(J), r = lim_r(J);
     int SK = 0, ok = 0;
     if (KIND == 1) {
-      SK = K == 0 ? 1 : (K == 1 ? kWin : kWin * kWin);
+      SK = U * (K == 0 ? 1 : (K == 1 ? kWin : kWin * kWin));
       ok = order_rt(ck, lim3(K), lim1(K));
     }
     T p = j0 > 0 ? win[w0 + 2 * (j0 - 1) * S] : T(0);
     T a = win[w0 + 2 * j0 * S], b = win[w0 + 2 * (j0 + 1) * S];
-    T c = j0 + 2 <= 8 ? win[w0 + 2 * (j0 + 2) * S] : T(0);
+    T c = j0 + 2 <= N ? win[w0 + 2 * (j0 + 2) * S] : T(0);
 #pragma unroll 1
-    for (int j = j0; j < j1 && 2 * j + 1 < r; ++j) {
+    for (int j = j0; j < j1 && (2 * j + 1) * U < r; ++j) {
       const int wi = w0 + (2 * j + 1) * S;
-      const int oj = order_rt(2 * j + 1, l3, l1);
+      const int oj = order_rt((2 * j + 1) * U, l3, l1);
       const T lj = window_line<KIND != 2>(oj, p, a, b, c);
       T pred = lj;
       if (KIND == 1) {
@@ -636,29 +638,29 @@ struct LevelSweep {
           pred = F::sub(F::add(win[wi - SK], win[wi - S]), win[wi - SK - S]);
         }
       }
-      emit_at(wi, cw0 + (2 * j + 1) * cs, own, pred);
+      emit_at(wi, cw0 + (2 * j + 1) * U * cs, own, pred);
       p = a;
       a = b;
       b = c;
-      if (j + 3 <= 8) c = win[w0 + 2 * (j + 3) * S];
+      if (j + 3 <= N) c = win[w0 + 2 * (j + 3) * S];
     }
   }
   // md cube points (x odd, cy, cz) along x with cube_at's full case order
   __device__ __forceinline__ void edge_cube_job(int cy, int cz, int j0, int j1) const {
     using E = Expr<T>;
     using F = Fp<T>;
-    constexpr int SY = kWin, SZ = kWin * kWin;
+    constexpr int SX = U, SY = U * kWin, SZ = U * kWin * kWin;
     const int w0 = (cz * kWin + cy) * kWin, cw0 = (cz * 16 + cy) * 16;
     const int oy = order_rt(cy, lim3(1), lim1(1)), oz = order_rt(cz, lim3(2), lim1(2));
     const int l3 = lim3(0), l1 = lim1(0), r = lim_r(0);
-    T p = j0 > 0 ? win[w0 + 2 * (j0 - 1)] : T(0);
-    T a = win[w0 + 2 * j0], b = win[w0 + 2 * (j0 + 1)];
-    T c = j0 + 2 <= 8 ? win[w0 + 2 * (j0 + 2)] : T(0);
+    T p = j0 > 0 ? win[w0 + 2 * (j0 - 1) * SX] : T(0);
+    T a = win[w0 + 2 * j0 * SX], b = win[w0 + 2 * (j0 + 1) * SX];
+    T c = j0 + 2 <= N ? win[w0 + 2 * (j0 + 2) * SX] : T(0);
 #pragma unroll 1
-    for (int j = j0; j < j1 && 2 * j + 1 < r; ++j) {
-      const int wi = w0 + 2 * j + 1;
+    for (int j = j0; j < j1 && (2 * j + 1) * U < r; ++j) {
+      const int wi = w0 + (2 * j + 1) * SX;
       const T* w = win + wi;
-      const int ox = order_rt(2 * j + 1, l3, l1);
+      const int ox = order_rt((2 * j + 1) * U, l3, l1);
       auto cy_ = [&]() { return E::cubic_lambda(w[-3 * SY], w[-SY], w[SY], w[3 * SY], nat); };
       auto cz_ = [&]() { return E::cubic_lambda(w[-3 * SZ], w[-SZ], w[SZ], w[3 * SZ], nat); };
       auto cx_ = [&]() { return E::cubic_lambda(p, a, b, c, nat); };
@@ -674,12 +676,79 @@ struct LevelSweep {
       else if (ox == 2) pred = E::quad_r_cube(a, b, c);
       else if (ox == 1) pred = E::lin(a, b);
       else pred = a;
-      emit_at(wi, cw0 + 2 * j + 1, true, pred);
+      emit_at(wi, cw0 + (2 * j + 1) * U, true, pred);
       p = a;
       a = b;
       b = c;
-      if (j + 3 <= 8) c = win[w0 + 2 * (j + 3)];
+      if (j + 3 <= N) c = win[w0 + 2 * (j + 3) * SX];
     }
+  }
+  // Level 1 (unit 2, four odd points per line) of any tile by half-line jobs
+  // with the runtime orders; not the last level, so every point in the field
+  // is predicted.  md: 150 line, 120 face and 32 cube jobs; per axis: 50,
+  // 90 and 162 jobs.
+  __device__ __forceinline__ void mid_md_jobs() const {
+    static_assert(U == 2, "level 1");
+    const int t = threadIdx.x;
+    auto kS = [](int a) { return a == 0 ? 1 : (a == 1 ? kWin : kWin * kWin); };
+    auto kC = [](int a) { return a == 0 ? 1 : (a == 1 ? 16 : 256); };
+    if (t < 150) {
+      const int h = t / 75, r = t - 75 * h, f = r / 25, l = r - 25 * f, u = 4 * (l % 5), v = 4 * (l / 5);
+      const int P = f == 0 ? 1 : 0, Q = f == 2 ? 1 : 2;
+      if (u < lim_r(P) && v < lim_r(Q))
+        edge_job<0>(u * kS(P) + v * kS(Q), f, 0, u * kC(P) + v * kC(Q), kC(f), (u | v) < 16, 2 * h, 2 * h + 2, 0);
+    }
+    __syncthreads();
+    if (t < 120) {
+      const int h = t / 60, r = t - 60 * h, f = r / 20, l = r - 20 * f, ce = 4 * (l % 5), ck = 4 * (l / 5) + 2;
+      const int J = f == 0 ? 1 : 0, K = f == 1 ? 2 : (f == 0 ? 2 : 1);
+      if (ce < lim_r(f) && ck < lim_r(K))
+        edge_job<1>(ce * kS(f) + ck * kS(K), J, K, ce * kC(f) + ck * kC(K), kC(J), ce < 16, 2 * h, 2 * h + 2, ck);
+    }
+    __syncthreads();
+    if (t < 32) {
+      const int line = t >> 1, h = t & 1, cy = 4 * (line & 3) + 2, cz = 4 * (line >> 2) + 2;
+      if (cy < lim_r(1) && cz < lim_r(2)) edge_cube_job(cy, cz, 2 * h, 2 * h + 2);
+    }
+    __syncthreads();
+  }
+  __device__ __forceinline__ void mid_axis_jobs(bool rev) const {
+    static_assert(U == 2, "level 1");
+    constexpr int SY = kWin, SZ = kWin * kWin;
+    const int t = threadIdx.x;
+    const int r0 = lim_r(0), r1 = lim_r(1), r2 = lim_r(2);
+    if (!rev) {  // z at (x, y) even; y at (x even, z any); x at (y, z any)
+      if (t < 50) {
+        const int h = t / 25, l = t - 25 * h, x = 4 * (l % 5), y = 4 * (l / 5);
+        if (x < r0 && y < r1) edge_job<2>(x + y * SY, 2, 0, x + 16 * y, 256, (x | y) < 16, 2 * h, 2 * h + 2, 0);
+      }
+      __syncthreads();
+      if (t < 90) {
+        const int h = t / 45, l = t - 45 * h, x = 4 * (l % 5), z = 2 * (l / 5);
+        if (x < r0 && z < r2) edge_job<2>(x + z * SZ, 1, 0, x + 256 * z, 16, (x | z) < 16, 2 * h, 2 * h + 2, 0);
+      }
+      __syncthreads();
+      if (t < 162) {
+        const int h = t / 81, l = t - 81 * h, y = 2 * (l % 9), z = 2 * (l / 9);
+        if (y < r1 && z < r2) edge_job<2>(y * SY + z * SZ, 0, 0, 16 * y + 256 * z, 1, (y | z) < 16, 2 * h, 2 * h + 2, 0);
+      }
+    } else {  // x at (y, z) even; y at (x any, z even); z at (x, y any)
+      if (t < 50) {
+        const int h = t / 25, l = t - 25 * h, y = 4 * (l % 5), z = 4 * (l / 5);
+        if (y < r1 && z < r2) edge_job<2>(y * SY + z * SZ, 0, 0, 16 * y + 256 * z, 1, (y | z) < 16, 2 * h, 2 * h + 2, 0);
+      }
+      __syncthreads();
+      if (t < 90) {
+        const int h = t / 45, l = t - 45 * h, x = 2 * (l % 9), z = 4 * (l / 9);
+        if (x < r0 && z < r2) edge_job<2>(x + z * SZ, 1, 0, x + 256 * z, 16, (x | z) < 16, 2 * h, 2 * h + 2, 0);
+      }
+      __syncthreads();
+      if (t < 162) {
+        const int h = t / 81, l = t - 81 * h, x = 2 * (l % 9), y = 2 * (l / 9);
+        if (x < r0 && y < r1) edge_job<2>(x + y * SY, 2, 0, x + 16 * y, 256, (x | y) < 16, 2 * h, 2 * h + 2, 0);
+      }
+    }
+    __syncthreads();
   }
   __device__ __forceinline__ void edge_md_lines() const {
     const int t = threadIdx.x;
@@ -810,6 +879,11 @@ struct LevelSweep {
   __device__ __forceinline__ void run(bool md, bool rev) const {
     constexpr bool kLast = U == 1;
     // axis codes: x = 0, y = 1, z = 2; AXES = a0 | a1 << 2 | a2 << 4
+    if constexpr (U == 2) {
+      if (md) mid_md_jobs();
+      else mid_axis_jobs(rev);
+      return;
+    }
     if constexpr (U == 1) {
       if constexpr (EDGE) {
         if (md) edge_md_lines();
