@@ -16,7 +16,9 @@ import oracle as O
 
 pytestmark = pytest.mark.gpu
 
-SHAPES = [(70, 45, 33), (50, 50, 50), (33, 66, 40)]
+# last-slab extents 6/13/1, 2, 2/8; all multiples of 16 (full-size edge
+# tiles, as in 384x384x256); 1 and 16 (no interior tile along z)
+SHAPES = [(70, 45, 33), (50, 50, 50), (33, 66, 40), (48, 32, 64), (17, 33, 16)]
 FLAGS = {
     "md": ([1, 1, 1, 1], [0, 0, 0, 0]),
     "axis": ([0, 0, 0, 0], [0, 0, 0, 0]),
