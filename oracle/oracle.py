@@ -180,6 +180,25 @@ def predict(data, eb, use_md, reverse, rel_eb):
     return anchors, qc, scratch
 
 
+def reconstruct(qc, anchors, shape, dtype, eb, use_md, reverse, rel_eb, maxlevel=4, old=None):
+    """Reconstruction from level-major codes and anchors (or_reconstruct, the
+    reference's interpolation_reverse / interpolation_progressive_reverse);
+    `old` selects the progressive form."""
+    nz, ny, nx = shape
+    dtype = np.dtype(dtype)
+    g = geometry(nx, ny, nz, dtype.itemsize)
+    p = intp(use_md, reverse)
+    p.alpha = lib_alpha(rel_eb)
+    qc = np.ascontiguousarray(qc, dtype=np.int32)
+    anchors = np.ascontiguousarray(anchors, dtype=dtype)
+    o = None if old is None else np.ascontiguousarray(old, dtype=dtype)
+    out = np.zeros(shape, dtype=dtype)
+    getattr(lib(), "or_reconstruct_" + _suffix(dtype))(
+        _p(qc), _p(anchors), C.byref(g), C.c_double(eb), C.byref(p), C.c_int(maxlevel),
+        _p(o) if o is not None else None, _p(out))
+    return out
+
+
 def lib_alpha(rel_eb):
     f = lib().or_alpha
     f.restype = C.c_double

@@ -76,23 +76,27 @@ def test_predict_and_reconstruct_forced_flags(env, dims, dtype, flag_name):
     assert np.array_equal(anchors[:na].cpu().numpy().view(np.uint8), o_anchors.view(np.uint8))
     assert np.array_equal(codes[:n].cpu().numpy(), o_qc[:n]), "codes differ from the oracle"
 
-    # full reconstruction from the codes against the oracle's decompression
+    # reconstruction from the same codes against the oracle's (the full
+    # pipeline also passes the codes through the bit planes, whose last-block
+    # quirk alters some codes on some shapes; that path has its own tests)
     l = P.lib()
     out = torch.empty((nz, ny, nx), dtype=torch.from_numpy(data[:0]).dtype, device="cuda")
     st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
     h.check(l.prism_reconstruct(h.ptr, C.c_void_p(codes.data_ptr()), C.c_void_p(anchors.data_ptr()), data.itemsize,
                                 nx, ny, nz, C.c_double(eb), C.c_double(0.0), flags8, 4, None,
                                 C.c_void_p(out.data_ptr()), st), "prism_reconstruct")
-    cont, _, _ = O.compress(data, 0, eb, 1, force=O.intp(md, rv))
-    ref = O.decompress(cont, (nz, ny, nx), dtype, 0, eb)
+    ref = O.reconstruct(o_qc, o_anchors, (nz, ny, nx), dtype, eb, md, rv, 0.0)
     rec = out.cpu().numpy()
     assert np.array_equal(rec.view(np.uint8), ref.view(np.uint8)), "reconstruction differs from the oracle"
 
-    # the progressive form adds the previous values to the same reconstruction
-    old = torch.from_numpy(field(dims, dtype, 5)).cuda()
+    # the progressive form (previous values added), also at a lower maxlevel
+    old_np = field(dims, dtype, 5)
+    old = torch.from_numpy(old_np).cuda()
     out2 = torch.empty_like(out)
-    h.check(l.prism_reconstruct(h.ptr, C.c_void_p(codes.data_ptr()), C.c_void_p(anchors.data_ptr()), data.itemsize,
-                                nx, ny, nz, C.c_double(eb), C.c_double(0.0), flags8, 4, C.c_void_p(old.data_ptr()),
-                                C.c_void_p(out2.data_ptr()), st), "prism_reconstruct progressive")
-    expect = (rec + old.cpu().numpy()).astype(dtype)
-    assert np.array_equal(out2.cpu().numpy().view(np.uint8), expect.view(np.uint8))
+    for maxlevel in (4, 2):
+        h.check(l.prism_reconstruct(h.ptr, C.c_void_p(codes.data_ptr()), C.c_void_p(anchors.data_ptr()),
+                                    data.itemsize, nx, ny, nz, C.c_double(eb), C.c_double(0.0), flags8, maxlevel,
+                                    C.c_void_p(old.data_ptr()), C.c_void_p(out2.data_ptr()), st),
+                "prism_reconstruct progressive")
+        ref2 = O.reconstruct(o_qc, o_anchors, (nz, ny, nx), dtype, eb, md, rv, 0.0, maxlevel, old_np)
+        assert np.array_equal(out2.cpu().numpy().view(np.uint8), ref2.view(np.uint8)), f"maxlevel {maxlevel}"

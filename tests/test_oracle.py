@@ -117,3 +117,22 @@ def test_oracle_roundtrip_bound_random_shapes():
         assert np.abs(out.astype(np.float64) - data).max() <= 1e-2 + slack
         checked += 1
     assert checked >= 1
+
+
+def test_oracle_predictor_bound_every_shape():
+    """The predictor alone (codes straight back into the reconstruction, no
+    bit planes) honours the bound on every shape, including those where the
+    reference's last shuffle block alters codes; progressive reconstruction
+    at maxlevel 4 adds the previous values."""
+    rng = np.random.default_rng(9)
+    for shape in [(64, 32, 48), (16, 33, 17), (33, 45, 70), (5, 3, 129), (1, 1, 300)]:
+        for dtype in (np.float32, np.float64):
+            data = (rng.standard_normal(shape).cumsum(axis=2) * 0.1).astype(dtype)
+            for md, rv in (([1] * 4, [0] * 4), ([0] * 4, [1] * 4), ([0, 1, 0, 1], [1, 0, 0, 1])):
+                anchors, qc, _ = O.predict(data, 1e-3, md, rv, 0.0)
+                out = O.reconstruct(qc, anchors, shape, dtype, 1e-3, md, rv, 0.0)
+                slack = 8 * np.finfo(dtype).eps * float(np.abs(data).max())
+                assert np.abs(out.astype(np.float64) - data).max() <= 1e-3 + slack
+                old = np.ones(shape, dtype=dtype)
+                prog = O.reconstruct(qc, anchors, shape, dtype, 1e-3, md, rv, 0.0, 4, old)
+                assert np.array_equal(prog, (out + old).astype(dtype))
