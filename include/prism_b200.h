@@ -67,8 +67,12 @@ const char* prism_last_error(const prism_handle* h);
  * accumulators (order: extrema, autotune, predict, shuffle, encode, trailer,
  * strategy, decode, inverse shuffle, reconstruct), returns the stage count and
  * clears them when reset != 0.  No counterpart in the reference, which times
- * its stages with blocking GPUTimer pairs (include/utils/timer.hpp:21-30). */
+ * its stages with blocking GPUTimer pairs (include/utils/timer.hpp:21-30).
+ * prism_profile_stages times only the stages whose bit (1 << index, order
+ * above) is set in mask: each timing event drains the stream, so timing
+ * every stage costs a few microseconds per launch. */
 int prism_profile(prism_handle* h, int enable);
+int prism_profile_stages(prism_handle* h, uint32_t mask);
 int prism_stage_times(prism_handle* h, double* ms, int* counts, int n, int reset);
 /* Number of kernels this handle has launched. */
 uint64_t prism_launch_count(const prism_handle* h);

@@ -95,6 +95,7 @@ def lib():
         l.prism_server_poll.argtypes = [vp, u64, C.POINTER(i32)]
         l.prism_server_destroy.argtypes = [vp]
         l.prism_profile.argtypes = [vp, i32]
+        l.prism_profile_stages.argtypes = [vp, u32]
         l.prism_stage_times.argtypes = [vp, vp, vp, i32, i32]
         l.prism_launch_count.argtypes = [vp]
         l.prism_launch_count.restype = u64
@@ -114,7 +115,7 @@ EXPORTED = [
     "prism_batch_destroy", "prism_server_create", "prism_server_add_field", "prism_server_submit",
     "prism_server_wait", "prism_server_stats_get", "prism_server_destroy", "prism_statistics", "prism_server_poll",
     "prism_file_save", "prism_file_open", "prism_file_step", "prism_file_info", "prism_file_close",
-    "prism_progressive_step_into",
+    "prism_progressive_step_into", "prism_profile_stages",
 ]
 
 STAGES = ["extrema", "autotune", "predict", "shuffle", "encode", "trailer", "strategy", "decode",
@@ -142,8 +143,13 @@ class Handle:
             msg = lib().prism_last_error(self.ptr)
             raise PrismError(f"{what}: {_STATUS.get(rc, rc)}: {msg.decode() if msg else ''}")
 
-    def profile(self, enable=True):
-        self.check(lib().prism_profile(self.ptr, int(enable)), "prism_profile")
+    def profile(self, enable=True, stages=None):
+        """Stage timing on/off; `stages` (names from STAGES) limits it to those."""
+        if stages is None:
+            self.check(lib().prism_profile(self.ptr, int(enable)), "prism_profile")
+        else:
+            mask = sum(1 << STAGES.index(s) for s in stages) if enable else 0
+            self.check(lib().prism_profile_stages(self.ptr, mask), "prism_profile_stages")
 
     def stage_times(self, reset=True):
         ms = (C.c_double * 16)()

@@ -387,11 +387,17 @@ inverse_last_block_kernel(const uint8_t* __restrict__ planes, int32_t* __restric
 // (0 for anchors and past n).  This fills the ranges the bulk shuffle does not
 // write; the last-block kernel then overwrites what it writes.
 struct ByteRange { uint64_t start, len; };
+// at most 32 planes x 4 levels + the tail, passed by value (kernel parameter
+// space) so that no host-to-device copy precedes the launch
+constexpr int kMaxRanges = 160;
+struct RangeList {
+  ByteRange r[kMaxRanges];
+};
 
 __global__ void leftover_fill_kernel(uint8_t* __restrict__ planes, const int32_t* __restrict__ qc, Geometry g,
-                                     const ByteRange* __restrict__ ranges, int nranges) {
+                                     const RangeList ranges, int nranges) {
   for (int r = blockIdx.x; r < nranges; r += gridDim.x) {
-    ByteRange br = ranges[r];
+    ByteRange br = ranges.r[r];
     for (uint64_t o = threadIdx.x; o < br.len; o += blockDim.x) {
       uint64_t b = br.start + o;
       uint64_t i = b >> 2;

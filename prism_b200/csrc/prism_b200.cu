@@ -99,7 +99,7 @@ struct prism_handle {
   std::string err;
   int sm_count = 148;
   uint64_t launches = 0;       // kernels launched by this handle
-  bool prof = false;
+  uint32_t prof = 0;  // bit i: time stage i
   // per stage, one event pair per launch since the last collection (steps
   // are enqueued back to back, so several launches of a stage can be pending)
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[kStCount];
@@ -120,6 +120,10 @@ struct prism_handle {
   // first step and reused by the later ones
   DevBuf prog_offs[64];
   size_t zero_anchors_ready = 0;  // leading bytes of zero_anchors known to be zero
+  // dimensions whose auto-tune sample windows `wins` holds (the windows
+  // depend on the dimensions only; uploading them from pageable memory would
+  // make the host wait for the stream at every compression)
+  uint32_t wins_dims[3] = {0, 0, 0};
 };
 
 constexpr int kProgSlotBytes = 128;  // StrategyState + error flag
@@ -163,7 +167,7 @@ static cudaError_t fork_join(prism_handle* h, cudaStream_t st, bool have_interio
 }
 
 static void prof_begin(prism_handle* h, int stage, cudaStream_t st) {
-  if (!h->prof) return;
+  if (!((h->prof >> stage) & 1u)) return;
   auto& v = h->ev[stage];
   if (h->ev_used[stage] == (int)v.size()) {
     cudaEvent_t a = nullptr, b = nullptr;
@@ -178,7 +182,7 @@ static void prof_begin(prism_handle* h, int stage, cudaStream_t st) {
   h->ev_used[stage] += 1;
 }
 static void prof_end(prism_handle* h, int stage, cudaStream_t st) {
-  if (!h->prof || h->ev_used[stage] == 0) return;
+  if (!((h->prof >> stage) & 1u) || h->ev_used[stage] == 0) return;
   cudaEventRecord(h->ev[stage][h->ev_used[stage] - 1].second, st);
 }
 // fold the recorded stage times into the accumulators (waits for them)
@@ -363,8 +367,13 @@ static int launch_autotune_params(prism_handle* h, const T* in, const Geometry& 
   if (!force_flags_dev) {
     CKA(h->part.ensure(sizeof(T) * 15 * std::max(nwin, 1) + 64));
     if (nwin > 0) {
-      CKA(h->wins.ensure(sizeof(SampleWindow) * nwin));
-      CK(cudaMemcpyAsync(h->wins.p, wins.data(), sizeof(SampleWindow) * nwin, cudaMemcpyHostToDevice, st));
+      if (h->wins_dims[0] != g.nx || h->wins_dims[1] != g.ny || h->wins_dims[2] != g.nz) {
+        CKA(h->wins.ensure(sizeof(SampleWindow) * nwin));
+        CK(cudaMemcpyAsync(h->wins.p, wins.data(), sizeof(SampleWindow) * nwin, cudaMemcpyHostToDevice, st));
+        h->wins_dims[0] = g.nx;
+        h->wins_dims[1] = g.ny;
+        h->wins_dims[2] = g.nz;
+      }
       prof_begin(h, kStAutotune, st);
       autotune_kernel<T><<<dim3(nwin, 6), kAttThreads, 0, st>>>(in, g, h->wins.as<SampleWindow>(), h->part.as<T>());
       prof_end(h, kStAutotune, st);
@@ -411,13 +420,11 @@ static int launch_bitshuffle(prism_handle* h, const int32_t* qc, const Geometry&
                              cudaStream_t st) {
   int64_t start_last = (g.sh_grid - 1) * (int64_t)kChunk;
   ShufPlan plan = make_shuf_plan(g, start_last);
-  ByteRange rng[160];
-  int nr = fill_ranges(g, plan, rng, 160);
+  RangeList rng;
+  int nr = fill_ranges(g, plan, rng.r, kMaxRanges);
   prof_begin(h, kStShuffle, st);
   if (nr > 0) {
-    CKA(h->ranges.ensure(sizeof(rng)));
-    CK(cudaMemcpyAsync(h->ranges.p, rng, sizeof(ByteRange) * nr, cudaMemcpyHostToDevice, st));
-    leftover_fill_kernel<<<nr, 256, 0, st>>>(planes, qc, g, h->ranges.as<ByteRange>(), nr);
+    leftover_fill_kernel<<<nr, 256, 0, st>>>(planes, qc, g, rng, nr);
     h->launches += 1;
   }
   const int32_t* codes = qc + g.anchors;
@@ -671,7 +678,13 @@ const char* prism_last_error(const prism_handle* h) { return h ? h->err.c_str() 
 
 int prism_profile(prism_handle* h, int enable) {
   if (!h) return PRISM_ERR_ARG;
-  h->prof = enable != 0;
+  h->prof = enable ? (1u << kStCount) - 1u : 0u;
+  return PRISM_OK;
+}
+
+int prism_profile_stages(prism_handle* h, uint32_t mask) {
+  if (!h) return PRISM_ERR_ARG;
+  h->prof = mask & ((1u << kStCount) - 1u);
   return PRISM_OK;
 }
 
