@@ -1056,6 +1056,10 @@ struct CompressSmem {
 };
 static_assert(sizeof(float) * kWinVol >= sizeof(uint64_t) * kRowTable, "row table fits the window");
 
+template <class T> struct PairOf;
+template <> struct PairOf<double> { using type = double2; };
+template <> struct PairOf<float> { using type = float2; };
+
 // Shared memory of a reconstruction tile: the window (codes travel in the
 // window slots) and the row table (~43 KB for double, ~23 KB for float).
 template <class T>
@@ -1173,6 +1177,41 @@ reconstruct_kernel(const int32_t* __restrict__ qc, const T* __restrict__ anchors
   }
   __syncthreads();
   sweep_levels<T, false, EDGE>(sm.win, nullptr, f.lim, f.last[2], sm.p);
+  if constexpr (!EDGE) {
+    // An interior tile writes 256 full rows of 16 values.  When every row
+    // start is aligned to a pair of values (even row stride, aligned
+    // buffers), pairs move as one vector: 2048 pairs, four in flight per
+    // thread, pair q at x = 2 (q % 8), y = q / 8 % 16, z = q / 128.
+    using V = typename PairOf<T>::type;
+    const uintptr_t ends = reinterpret_cast<uintptr_t>(out + base) | (PROG ? reinterpret_cast<uintptr_t>(old + base) : 0);
+    const bool pairs = (sy & 1) == 0 && ends % sizeof(V) == 0;
+    if (pairs) {
+      for (int b = tid; b < 2048; b += 4 * kPredThreads) {
+        V o[4];
+        if (PROG) {
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            const int q = b + k * kPredThreads, x = 2 * (q & 7), y = (q >> 3) & 15, z = q >> 7;
+            o[k] = *reinterpret_cast<const V*>(old + base + x + (uint64_t)y * sy + (uint64_t)z * sz);
+          }
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const int q = b + k * kPredThreads, x = 2 * (q & 7), y = (q >> 3) & 15, z = q >> 7;
+          const int wi = (z * kWin + y) * kWin + x;
+          V v;
+          v.x = sm.win[wi];
+          v.y = sm.win[wi + 1];
+          if (PROG) {
+            v.x = Fp<T>::add(v.x, o[k].x);
+            v.y = Fp<T>::add(v.y, o[k].y);
+          }
+          *reinterpret_cast<V*>(out + base + x + (uint64_t)y * sy + (uint64_t)z * sz) = v;
+        }
+      }
+      return;
+    }
+  }
   const int xs = 16 + (EDGE && f.last[0]), ys = 16 + (EDGE && f.last[1]), zs = 16 + (EDGE && f.last[2]);
   const int total = xs * ys * zs;
   for (int b = tid; b < total; b += kPrefetch * kPredThreads) {
