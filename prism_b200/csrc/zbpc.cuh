@@ -458,7 +458,7 @@ __device__ __forceinline__ void copy_in(uint8_t* dst, const uint8_t* src, int n)
 // decoded from its tail: bitmap 4 B -> 32 B -> 256 B -> 2048 B (fill-forward:
 // byte i = kept byte rank(i) - 1, rank the inclusive flag count), then the
 // nonzero bytes are scattered by the zero-elimination bitmap.
-__global__ void __launch_bounds__(kZThreads)
+__global__ void __launch_bounds__(kZThreads, 4)
 zbpc_decode_kernel(const uint8_t* __restrict__ stream, uint64_t stream_bytes, const int64_t* __restrict__ offs,
                    Geometry g, uint8_t* __restrict__ planes, const int* __restrict__ begin,
                    const int* __restrict__ end, int* __restrict__ error_flag) {
