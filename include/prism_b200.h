@@ -163,9 +163,10 @@ int prism_lossless_encode(prism_handle* h, const uint8_t* d_planes, uint32_t nx,
                           uint32_t nz, uint8_t* d_stream, uint64_t capacity, uint64_t* size_out,
                           uint64_t comp_size_bp[128], void* stream);
 /* Lossless stream -> planes.  With begin/end (host, both or neither), only
- * the chunks of planes [begin[3-l], end[3-l]) of each level are decoded and
- * the chunks of every other plane are written as zeros, as a progressive
- * step needs them. */
+ * the chunks of planes [begin[3-l], end[3-l]) of each level are decoded; of
+ * the other planes, the bytes that the inverse shuffle of the selected planes
+ * reads (their device placement reaches into neighbouring host planes) are
+ * written as zeros and the rest of the buffer is left as it is. */
 int prism_lossless_decode(prism_handle* h, const uint8_t* d_stream, uint32_t nx, uint32_t ny,
                           uint32_t nz, const int begin[4], const int end[4], uint8_t* d_planes,
                           void* stream);

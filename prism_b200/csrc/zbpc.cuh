@@ -474,13 +474,22 @@ zbpc_decode_kernel(const uint8_t* __restrict__ stream, uint64_t stream_bytes, co
       int64_t cpp = g.chunks_level[loc.level] >> 5;
       int64_t real = loc.plane * cpp + loc.offset;
       if (real < begin[3 - loc.level] * cpp || real >= end[3 - loc.level] * cpp) {
-        // a plane this step does not load reads as zero (chunk sizes and
-        // offsets are multiples of 8, and the chunks tile the plane buffer)
-        const int b0 = tid * 32;
-        if (b0 < loc.osize) {
-          uint2* d2 = reinterpret_cast<uint2*>(planes + loc.base + b0);
-          const int nq = min(4, (loc.osize - b0) >> 3);
-          for (int q = 0; q < nq; ++q) d2[q] = make_uint2(0, 0);
+        // A plane this step does not load reads as zero where the inverse
+        // shuffle reads it: the inverse reads, per level l, the planes
+        // [lo, hi) it selects at their device placement, bytes
+        // [daprefix[l] + lo dstride[l], daprefix[l] + hi dstride[l]), which
+        // can reach into the host placement of neighbouring planes.  Only the
+        // part of this chunk inside those ranges is zeroed (all bounds are
+        // multiples of 8); the rest is never read.
+        const int64_t cb = loc.base, ce = loc.base + loc.osize;
+#pragma unroll 1
+        for (int l = 0; l < 4; ++l) {
+          const int lo = begin[3 - l], hi = end[3 - l];
+          if (lo >= hi) continue;
+          const int64_t r0 = g.daprefix[l] + (int64_t)lo * g.dstride[l], r1 = g.daprefix[l] + (int64_t)hi * g.dstride[l];
+          const int64_t a = cb > r0 ? cb : r0, e = ce < r1 ? ce : r1;
+          for (int64_t o = a + 8 * (int64_t)tid; o < e; o += 8 * (int64_t)kZThreads)
+            *reinterpret_cast<uint2*>(planes + o) = make_uint2(0, 0);
         }
         continue;
       }
