@@ -240,7 +240,10 @@ __device__ __forceinline__ int32_t quantize(T orig, T pred, T ebr, T ebx2, T* re
   int qi = F::to_int_rz(F::mul(code, T(0.5)));
   T qt = F::from_int(qi);
   *rec = F::fma(qt, ebx2, pred);
-  return F::to_int_rz(qt);
+  // the code is (int)qt: qi itself for double (every int is exact there);
+  // float rounds |qi| > 2^24, so it converts back
+  if constexpr (sizeof(T) == 8) return qi;
+  else return F::to_int_rz(qt);
 }
 
 constexpr int kPredThreads = 256;
