@@ -102,6 +102,25 @@ def test_progressive_out_of_place_reference_container(env, name):
     prog.close()
 
 
+def test_progressive_step_into_arguments(env):
+    """The out-of-place step accepts no previous buffer on the first step only,
+    and rejects a non-positive target."""
+    torch, P, h = env
+    name = SMALL_PROG[0]
+    comp = P.Compressor(ctx_of(P, name), h)
+    cont = to_dev(torch, np.frombuffer(gu.raw(name, "cmp.bin"), np.uint8))
+    prog = comp.progressive(cont)
+    l, st = P.lib(), C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    out = torch.empty_like(prog.values)
+    t0 = gu.CASES[name]["targets"][0]
+    assert l.prism_progressive_step_into(prog.ptr, 0.0, None, C.c_void_p(out.data_ptr()), st) == -1
+    assert l.prism_progressive_step_into(prog.ptr, t0, None, C.c_void_p(out.data_ptr()), st) == 0
+    prog.state()
+    assert gu.sha(out.cpu().numpy()) == gu.digests(name)["prog0.bin"][1]
+    assert l.prism_progressive_step_into(prog.ptr, t0, None, C.c_void_p(out.data_ptr()), st) == -1
+    prog.close()
+
+
 RANDOM_SHAPES = [(40, 23, 17), (70, 45, 33), (129, 3, 5), (300, 41, 1), (2000, 1, 1), (16, 16, 16), (17, 17, 17),
                  (48, 48, 48)]
 
