@@ -259,6 +259,12 @@ __device__ __forceinline__ void copy_async(void* smem_dst, const void* gmem_src)
   asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(gmem_src), "n"(BYTES) : "memory");
 }
 __device__ __forceinline__ void copy_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+__device__ __forceinline__ void copy_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// wait until at most N of this thread's committed groups are still in flight
+template <int N>
+__device__ __forceinline__ void copy_async_wait_group() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
 __device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 
 // ---- tile sweep --------------------------------------------------------------
@@ -937,12 +943,25 @@ __device__ __forceinline__ void sweep_level(T* win, int32_t* cw, const AxisLimit
 }
 
 // spline_layout_interpolate (:1771-2027): levels 3..0
+// in two parts: levels 3..1 only touch the 9^3 window points whose
+// coordinates are all even, level 0 the rest as well
 template <class T, bool COMPRESS, bool EDGE>
-__device__ void sweep_levels(T* win, int32_t* cw, const AxisLimits& lim, bool zlast, const PredParams<T>& p) {
+__device__ void sweep_coarse(T* win, int32_t* cw, const AxisLimits& lim, bool zlast, const PredParams<T>& p) {
   sweep_level<T, COMPRESS, EDGE, 8, 3>(win, cw, lim, zlast, p);
   sweep_level<T, COMPRESS, EDGE, 4, 2>(win, cw, lim, zlast, p);
   sweep_level<T, COMPRESS, EDGE, 2, 1>(win, cw, lim, zlast, p);
+}
+template <class T, bool COMPRESS, bool EDGE>
+__device__ void sweep_fine(T* win, int32_t* cw, const AxisLimits& lim, bool zlast, const PredParams<T>& p) {
   sweep_level<T, COMPRESS, EDGE, 1, 0>(win, cw, lim, zlast, p);
+}
+
+// window index of the j-th of the 9^3 points with all coordinates even
+__device__ __forceinline__ int even_point(int j, int& x, int& y, int& z) {
+  x = 2 * (j % 9);
+  y = 2 * ((j / 9) % 9);
+  z = 2 * (j / 81);
+  return (z * kWin + y) * kWin + x;
 }
 
 // ---- tiles -------------------------------------------------------------------
@@ -1090,17 +1109,31 @@ __device__ __forceinline__ void compress_tile(CompressSmem<T>& sm, const T* __re
   if (tid == 0) sm.p = *pp;
   const uint64_t sy = g.nx, sz = (uint64_t)g.nx * g.ny;
   const T* base = data + (uint64_t)f.gs[0] + (uint64_t)f.gs[1] * sy + (uint64_t)f.gs[2] * sz;
+  // two copy groups: the points levels 3..1 use, then the rest, which
+  // arrive while those levels run
+  for (int j = tid; j < 729; j += kPredThreads) {
+    int x, y, z;
+    const int i = even_point(j, x, y, z);
+    if (L.in_data(x, y, z)) copy_async<sizeof(T)>(&sm.win[i], base + x + (uint64_t)y * sy + (uint64_t)z * sz);
+    else sm.win[i] = T(0);
+  }
+  copy_async_commit();
 #pragma unroll 4
   for (int i = tid; i < kWinVol; i += kPredThreads) {
     int x, y, z;
     win_xyz(i, x, y, z);
+    if (((x | y | z) & 1) == 0) continue;
     if (L.in_data(x, y, z)) copy_async<sizeof(T)>(&sm.win[i], base + x + (uint64_t)y * sy + (uint64_t)z * sz);
     else sm.win[i] = T(0);
   }
-  copy_async_wait_all();
+  copy_async_commit();
+  copy_async_wait_group<1>();
   __syncthreads();
   if (tid == 0) anchors[bi[0] + (uint64_t)bi[1] * g.ax + (uint64_t)bi[2] * g.ax * g.ay] = sm.win[0];
-  sweep_levels<T, true, EDGE>(sm.win, sm.cw, f.lim, f.last[2], sm.p);
+  sweep_coarse<T, true, EDGE>(sm.win, sm.cw, f.lim, f.last[2], sm.p);
+  copy_async_wait_group<0>();
+  __syncthreads();
+  sweep_fine<T, true, EDGE>(sm.win, sm.cw, f.lim, f.last[2], sm.p);
   // Every non-anchor point of the tile's own 16^3 that lies in the field was
   // emitted (on a last tile the plane at 16 lies outside the field).
   __syncthreads();
@@ -1160,17 +1193,29 @@ reconstruct_kernel(const int32_t* __restrict__ qc, const T* __restrict__ anchors
   }
   __syncthreads();
   // each code lands in the low word of its window slot (converted when its
-  // point is predicted); every other slot reads as zero
-#pragma unroll 4
-  for (int i = tid; i < kWinVol; i += kPredThreads) {
+  // point is predicted); every other slot reads as zero.  Two copy groups:
+  // the codes of levels 3..1 (points with all coordinates even), then the
+  // level-0 codes, which arrive while levels 3..1 run.
+  for (int j = tid; j < 729; j += kPredThreads) {
     int x, y, z;
-    win_xyz(i, x, y, z);
+    const int i = even_point(j, x, y, z);
     const int lv = win_level(x, y, z);
     int32_t* dst = reinterpret_cast<int32_t*>(&sm.win[i]);
     if (lv < 4 && lv <= maxlevel && L.in_data(x, y, z)) copy_async<4>(dst, qc + slot_of(sm.rows, lv, x, y, z));
     else sm.win[i] = T(0);
   }
-  copy_async_wait_all();
+  copy_async_commit();
+#pragma unroll 4
+  for (int i = tid; i < kWinVol; i += kPredThreads) {
+    int x, y, z;
+    win_xyz(i, x, y, z);
+    if (((x | y | z) & 1) == 0) continue;
+    int32_t* dst = reinterpret_cast<int32_t*>(&sm.win[i]);
+    if (maxlevel >= 0 && L.in_data(x, y, z)) copy_async<4>(dst, qc + slot_of(sm.rows, 0, x, y, z));
+    else sm.win[i] = T(0);
+  }
+  copy_async_commit();
+  copy_async_wait_group<1>();
   __syncthreads();
   if (tid < 8) {  // x_reset_scratch_data (:1027-1067): anchors at the corners
     int x = (tid & 1) * 16, y = ((tid >> 1) & 1) * 16, z = (tid >> 2) * 16;
@@ -1179,7 +1224,10 @@ reconstruct_kernel(const int32_t* __restrict__ qc, const T* __restrict__ anchors
       sm.win[(z * kWin + y) * kWin + x] = anchors[ax + (uint64_t)ay * g.ax + (uint64_t)az * g.ax * g.ay];
   }
   __syncthreads();
-  sweep_levels<T, false, EDGE>(sm.win, nullptr, f.lim, f.last[2], sm.p);
+  sweep_coarse<T, false, EDGE>(sm.win, nullptr, f.lim, f.last[2], sm.p);
+  copy_async_wait_group<0>();
+  __syncthreads();
+  sweep_fine<T, false, EDGE>(sm.win, nullptr, f.lim, f.last[2], sm.p);
   if constexpr (!EDGE) {
     // An interior tile writes 256 full rows of 16 values.  When every row
     // start is aligned to a pair of values (even row stride, aligned
