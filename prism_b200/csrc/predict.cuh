@@ -28,7 +28,7 @@ struct PredParams {
   T ebx2[4];       // 2*eb scaled per level
   uint8_t use_md[4];
   uint8_t reverse[4];
-  uint8_t natural[4];
+  uint8_t natural[4];  // always 0: the tile sweeps use the default cubic
   int32_t maxlevel;  // levels above are skipped (:1848-1849)
 };
 
@@ -379,7 +379,14 @@ struct LevelSweep {
   Limits<EDGE> L;
   bool zlast;  // the tile is the last along z (exclusive form allows z = 16)
   T ebr, ebx2;
-  bool nat;
+  // The tile sweeps evaluate the default cubic (nan_cubic_interp): the
+  // natural cubic is selected only by the reference's hidden `-cubic
+  // natural` test flag (parameters.cu:199-204), which this library does not
+  // offer (PredParams::natural is always 0; the auto-tuner still sums the
+  // natural candidate's errors with its own code).  A compile-time constant
+  // removes a branch per cubic and the unused form's division from every
+  // stage.
+  static constexpr bool nat = false;
 
   // The reconstruction keeps each point's code as an int32 in the low word of
   // the point's own window slot until the point is predicted (no prediction
@@ -499,31 +506,50 @@ struct LevelSweep {
   // KIND 1: md faces, the job axis J and a second odd axis with stride SK
   // and order ok (face_at: both cubic -> the mean of the two lines, one cubic
   // -> that line, neither -> the mean; add() is commutative bit for bit).
+  // Point j of a job with its order OJ along the job axis (interior orders:
+  // j = 0 quadratic from the right, j = 7 from the left, cubic in between).
+  template <int KIND, int OJ>
+  __device__ __forceinline__ void md_point(int j, int w0, int S, int cw0, int cs, bool own, int SK, int ok, T p,
+                                           T a, T b, T c) const {
+    using E = Expr<T>;
+    using F = Fp<T>;
+    const int wi = w0 + (2 * j + 1) * S;
+    const T lj = OJ == 4 ? (KIND == 2 ? E::cubic_axis(p, a, b, c, nat) : E::cubic_lambda(p, a, b, c, nat))
+                         : (OJ == 2 ? E::quad_r(a, b, c) : E::quad_l(p, a, b));
+    T pred = lj;
+    if (KIND == 1 && !(OJ == 4 && ok != 4)) {
+      const T lk = line_md_rt(win + wi, SK, ok);
+      pred = (OJ != 4 && ok == 4) ? lk : E::half(F::add(lj, lk));
+    }
+    emit_at(wi, cw0 + (2 * j + 1) * cs, own, pred);
+  }
+  // The first and last points are peeled off the loop, so inside it the
+  // order is a constant and a point costs no order branches.
   template <int KIND>
   __device__ __forceinline__ void md_job(int w0, int S, int cw0, int cs, bool own, int j0, int j1, int SK,
                                          int ok) const {
-    using E = Expr<T>;
-    using F = Fp<T>;
     T p = j0 > 0 ? win[w0 + 2 * (j0 - 1) * S] : T(0);
     T a = win[w0 + 2 * j0 * S], b = win[w0 + 2 * (j0 + 1) * S];
     T c = j0 + 2 <= 8 ? win[w0 + 2 * (j0 + 2) * S] : T(0);
+    int j = j0;
+    if (j == 0 && j < j1) {
+      md_point<KIND, 2>(0, w0, S, cw0, cs, own, SK, ok, p, a, b, c);
+      p = a;
+      a = b;
+      b = c;
+      c = win[w0 + 6 * S];
+      j = 1;
+    }
+    const int jm = j1 < 7 ? j1 : 7;
 #pragma unroll 1
-    for (int j = j0; j < j1; ++j) {
-      const int wi = w0 + (2 * j + 1) * S;
-      const int oj = j == 0 ? 2 : (j == 7 ? 3 : 4);
-      const T lj = oj == 4 ? (KIND == 2 ? E::cubic_axis(p, a, b, c, nat) : E::cubic_lambda(p, a, b, c, nat))
-                           : (oj == 2 ? E::quad_r(a, b, c) : E::quad_l(p, a, b));
-      T pred = lj;
-      if (KIND == 1 && !(oj == 4 && ok != 4)) {
-        const T lk = line_md_rt(win + wi, SK, ok);
-        pred = (oj != 4 && ok == 4) ? lk : E::half(F::add(lj, lk));
-      }
-      emit_at(wi, cw0 + (2 * j + 1) * cs, own, pred);
+    for (; j < jm; ++j) {
+      md_point<KIND, 4>(j, w0, S, cw0, cs, own, SK, ok, p, a, b, c);
       p = a;
       a = b;
       b = c;
       if (j + 3 <= 8) c = win[w0 + 2 * (j + 3) * S];
     }
+    if (j == 7 && j1 == 8) md_point<KIND, 3>(7, w0, S, cw0, cs, own, SK, ok, p, a, b, c);
   }
   // md cube points (x odd, cy, cz) along x, cube_at's cases for interior
   // orders with its summation order for three cubics
@@ -937,8 +963,7 @@ template <class T, bool COMPRESS, bool EDGE, int U, int LEVEL>
 __device__ __forceinline__ void sweep_level(T* win, int32_t* cw, const AxisLimits& lim, bool zlast,
                                             const PredParams<T>& p) {
   if (LEVEL > p.maxlevel) return;
-  LevelSweep<T, COMPRESS, U, EDGE> lv{win, cw, Limits<EDGE>{lim}, zlast, p.ebr[LEVEL], p.ebx2[LEVEL],
-                                      p.natural[LEVEL] != 0};
+  LevelSweep<T, COMPRESS, U, EDGE> lv{win, cw, Limits<EDGE>{lim}, zlast, p.ebr[LEVEL], p.ebx2[LEVEL]};
   lv.run(p.use_md[LEVEL] != 0, p.reverse[LEVEL] != 0);
 }
 

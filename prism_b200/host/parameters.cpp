@@ -104,7 +104,14 @@ int parse_argv(prism_context* c, int argc, char** argv) {
         }
       } else if (!strcmp(a, "-prog")) c->bt = NB;
       else if (!strcmp(a, "-cubic")) {
-        if (i + 1 < argc && !strcmp(argv[++i], "natural")) for (bool& v : c->intp_param.use_natural) v = true;
+        // The reference's hidden test flag switches its sweeps to the natural
+        // cubic (parameters.cu:199-204).  The library computes the default
+        // cubic only, so the flag is refused rather than ignored: ignoring it
+        // would write files that differ from the reference's.
+        if (i + 1 < argc && !strcmp(argv[++i], "natural")) {
+          std::cerr << "Error: -cubic natural is not supported (default cubic only)" << std::endl;
+          return 1;
+        }
       } else if (!strcmp(a, "-md")) {
         if (i + 1 < argc) {
           if (!strcmp(argv[i + 1], "true")) for (bool& v : c->intp_param.use_md) v = true;

@@ -55,3 +55,20 @@ def test_errors_are_status_codes_not_exits():
     size = C.c_uint64()
     rc = l.prism_compress(None, None, 4, 1, 1, 1, 0, 1e-3, 0, None, 0, C.byref(size), None, None)
     assert rc == -1
+
+
+def test_cli_refuses_natural_cubic(tmp_path):
+    """`-cubic natural` (a hidden test flag of the reference's CLI) would make
+    the reference write different bytes; the CLI refuses it before any GPU
+    work instead of ignoring it."""
+    import subprocess
+    cli = _build.build_cli()
+    if cli is None:
+        pytest.skip("CLI sources absent")
+    src = tmp_path / "f.f32"
+    src.write_bytes(b"\0" * 4 * 8 * 8 * 8)
+    p = subprocess.run([cli, "-i", str(src), "-f", "-3", "8", "8", "8", "-R", "1e-3", "-z", "-cubic", "natural"],
+                       capture_output=True, text=True, timeout=60)
+    assert p.returncode != 0
+    assert "-cubic natural is not supported" in p.stderr
+    assert not os.path.exists(str(src) + ".prisma")
