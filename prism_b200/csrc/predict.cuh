@@ -1230,14 +1230,27 @@ reconstruct_kernel(const int32_t* __restrict__ qc, const T* __restrict__ anchors
     else sm.win[i] = T(0);
   }
   copy_async_commit();
-#pragma unroll 4
-  for (int i = tid; i < kWinVol; i += kPredThreads) {
-    int x, y, z;
-    win_xyz(i, x, y, z);
-    if (((x | y | z) & 1) == 0) continue;
-    int32_t* dst = reinterpret_cast<int32_t*>(&sm.win[i]);
-    if (maxlevel >= 0 && L.in_data(x, y, z)) copy_async<4>(dst, qc + slot_of(sm.rows, 0, x, y, z));
-    else sm.win[i] = T(0);
+  // Level-0 codes by window rows r = z*17 + y: a row with y or z odd holds
+  // 17 level-0 points at consecutive slots rows[r] + x, a row with both even
+  // its 8 odd-x points at rows[r] + x/2.  Each half-warp takes x = 0..15 of
+  // one row (the row's slot base is one shared broadcast), then x = 16.
+  {
+    const int lane = tid & 31, x = lane & 15;
+    for (int r = (tid >> 5) * 2 + (lane >> 4); r < kWin * kWin; r += 2 * (kPredThreads / 32)) {
+      const int y = r % kWin, z = r / kWin;
+      const int ee = ((y | z) & 1) == 0;
+      if (ee && !(x & 1)) continue;
+      T* dst = &sm.win[r * kWin + x];
+      if (maxlevel >= 0 && L.in_data(x, y, z)) copy_async<4>(dst, qc + (sm.rows[r] + (uint64_t)(x >> ee)));
+      else *dst = T(0);
+    }
+    for (int r = tid; r < kWin * kWin; r += kPredThreads) {
+      const int y = r % kWin, z = r / kWin;
+      if (((y | z) & 1) == 0) continue;
+      T* dst = &sm.win[r * kWin + 16];
+      if (maxlevel >= 0 && L.in_data(16, y, z)) copy_async<4>(dst, qc + (sm.rows[r] + 16));
+      else *dst = T(0);
+    }
   }
   copy_async_commit();
   copy_async_wait_group<1>();
