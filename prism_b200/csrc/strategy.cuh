@@ -3,11 +3,12 @@
 // stays within floor(target*0.954/eb) - 1 while skipping the most bytes.
 //
 // The reference scans all 33^4 (b0, b1, b2, b3) combinations with 33 CTAs of
-// 1024 threads; the per-thread scan (strict >), the per-block tree reduction
-// (strict <, left kept) and the cross-block tree reduction define which of
-// several equal-valued choices wins, so this kernel keeps exactly that
-// structure.  The cross-block step runs as a second tiny kernel instead of the
-// reference's spin barrier.
+// 1024 threads; its per-thread scan (strict >), per-block tree reduction
+// (strict <, left kept) and cross-block tree reduction define which of
+// several equal-valued choices wins.  That choice is restated below as a
+// total order on the candidates, so the scan runs as 1188 small CTAs (one
+// per scan round and b0, filling the GPU) and a one-warp reduction instead
+// of 33 CTAs and the reference's spin barrier.
 #pragma once
 #include <stdint.h>
 
@@ -36,11 +37,6 @@ __device__ __forceinline__ uint64_t strategy_cost(int l, int b) {
   return (uint64_t)ceil(err);
 }
 
-struct StrategyBlock {
-  unsigned long long value;
-  int target[4];
-};
-
 // findStrategy_h (:179-208): the bound and target in absolute units
 __device__ __forceinline__ void strategy_setup(int mode, double bound, double target, const double* range,
                                                bool* use_search, uint64_t* target_cost) {
@@ -51,18 +47,44 @@ __device__ __forceinline__ void strategy_setup(int mode, double bound, double ta
   *target_cost = (uint64_t)floor(__ddiv_rn(scaled, eb)) - 1;
 }
 
-__global__ void __launch_bounds__(1024)
-strategy_search_kernel(const uint64_t* __restrict__ cs, int mode, double bound, double target,
-                       const double* __restrict__ range, StrategyBlock* __restrict__ out) {
+// Which candidate the reference's search returns.  Its block b0 scans, in
+// thread t, the positions pos = t + 1024 k in increasing k and keeps the
+// first maximum (strict >); a block then reduces its 1024 threads by the
+// interleaved tree (strides 512..1, the left entry kept on ties) and the 33
+// blocks reduce the same way.  Such a tree returns the maximum with ties
+// resolved towards the smallest bit-reversed index, so the winner is the
+// candidate of largest value (> 0, within the cost) with ties broken by
+// bit-reversed b0, then bit-reversed t, then k.  That order is packed into
+// `key` (larger wins), which lets any reduction order find it: here one CTA
+// per (k, b0), 1188 in all, and a final warp.
+constexpr int kStrategyRounds = (33 * 33 * 33 + 1023) / 1024;  // 36
+constexpr int kStrategyCells = kStrategyRounds * 33;
+
+struct StrategyBest {
+  unsigned long long value;
+  unsigned int key;  // (63 - brev6(b0)) << 16 | (1023 - brev10(t)) << 6 | (63 - k)
+  unsigned int pad;
+};
+
+__device__ __forceinline__ unsigned strategy_brev(unsigned v, int bits) { return __brev(v) >> (32 - bits); }
+
+__device__ __forceinline__ bool strategy_better(unsigned long long v, unsigned k, unsigned long long bv,
+                                                unsigned bk) {
+  return v > bv || (v == bv && k > bk);
+}
+
+__global__ void __launch_bounds__(256)
+strategy_scan_kernel(const uint64_t* __restrict__ cs, int mode, double bound, double target,
+                     const double* __restrict__ range, StrategyBest* __restrict__ out) {
   bool use_search;
   uint64_t target_cost;
   strategy_setup(mode, bound, target, range, &use_search, &target_cost);
   if (!use_search) return;
   __shared__ uint64_t cost[4][33];
   __shared__ uint64_t vt[4][33];
-  __shared__ unsigned long long maxv[1024];
-  __shared__ int maxt[1024];
-  const int tid = threadIdx.x, b0 = blockIdx.x;
+  __shared__ unsigned long long wv[8];
+  __shared__ unsigned wk[8];
+  const int tid = threadIdx.x, k = blockIdx.x, b0 = blockIdx.y;
   if (tid < 4 * 33) {
     int l = tid / 33, b = tid % 33;
     cost[l][b] = strategy_cost(l, b);
@@ -70,83 +92,76 @@ strategy_search_kernel(const uint64_t* __restrict__ cs, int mode, double bound, 
     vt[l][b] = b == 0 ? top : (b == 32 ? 0 : top - cs[l * 32 + b - 1]);
   }
   __syncthreads();
+  const unsigned kb = (63u - strategy_brev((unsigned)b0, 6)) << 16 | (63u - (unsigned)k);
   unsigned long long best = 0;
-  int r[4] = {32, 32, 32, 32};
-  for (int pos = tid; pos < 33 * 33 * 33; pos += 1024) {
-    int b1 = pos / (33 * 33), b2 = (pos / 33) % 33, b3 = pos % 33;
-    uint64_t tc = cost[0][b0] + cost[1][b1] + cost[2][b2] + cost[3][b3];
-    if (tc <= target_cost) {
-      unsigned long long v = vt[0][b0] + vt[1][b1] + vt[2][b2] + vt[3][b3];
-      if (v > best) { r[0] = b0; r[1] = b1; r[2] = b2; r[3] = b3; best = v; }
+  unsigned bkey = 0;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int t = q * 256 + tid, pos = k * 1024 + t;
+    if (pos < 33 * 33 * 33) {
+      const int b1 = pos / (33 * 33), b2 = (pos / 33) % 33, b3 = pos % 33;
+      const uint64_t tc = cost[0][b0] + cost[1][b1] + cost[2][b2] + cost[3][b3];
+      if (tc <= target_cost) {
+        const unsigned long long v = vt[0][b0] + vt[1][b1] + vt[2][b2] + vt[3][b3];
+        const unsigned key = kb | (1023u - strategy_brev((unsigned)t, 10)) << 6;
+        if (v > 0 && strategy_better(v, key, best, bkey)) { best = v; bkey = key; }
+      }
     }
   }
-  maxv[tid] = best;
-  maxt[tid] = tid;
+  const int lane = tid & 31, warp = tid >> 5;
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) {
+    const unsigned long long ov = __shfl_xor_sync(0xffffffffu, best, d);
+    const unsigned ok = __shfl_xor_sync(0xffffffffu, bkey, d);
+    if (strategy_better(ov, ok, best, bkey)) { best = ov; bkey = ok; }
+  }
+  if (lane == 0) { wv[warp] = best; wk[warp] = bkey; }
   __syncthreads();
-  for (int s = 512; s > 0; s >>= 1) {
-    if (tid < s && maxv[tid] < maxv[tid + s]) { maxv[tid] = maxv[tid + s]; maxt[tid] = maxt[tid + s]; }
-    __syncthreads();
-  }
-  if (tid == maxt[0]) {
-    out[b0].value = maxv[0];
-    for (int k = 0; k < 4; ++k) out[b0].target[k] = r[k];
+  if (tid == 0) {
+    for (int w = 1; w < 8; ++w)
+      if (strategy_better(wv[w], wk[w], best, bkey)) { best = wv[w]; bkey = wk[w]; }
+    StrategyBest r;
+    r.value = best;
+    r.key = bkey;
+    r.pad = 0;
+    out[b0 * kStrategyRounds + k] = r;
   }
 }
 
-// Cross-block reduction + begin/end/maxlevel update (dataloader.cu:278-334),
-// or loadall (:21-28) when the target is below the compression bound.
-__global__ void strategy_finish_kernel(const StrategyBlock* __restrict__ blk, int mode, double bound,
-                                       double target, const double* __restrict__ range,
-                                       StrategyState* __restrict__ st) {
-  if (threadIdx.x != 0) return;
-  bool use_search;
-  uint64_t target_cost;
-  strategy_setup(mode, bound, target, range, &use_search, &target_cost);
-  StrategyState s = *st;
-  int maxlevel = 4;
-  for (int i = 0; i < 4; ++i) s.begin[i] = s.end[i];
-  if (!use_search) {
-    for (int i = 0; i < 4; ++i) s.end[i] = 32;
-    maxlevel = s.begin[0] < 32 ? 3 : s.begin[1] < 32 ? 2 : s.begin[2] < 32 ? 1 : s.begin[3] < 32 ? 0 : 4;
-  } else {
-    unsigned long long v[64];
-    int bid[64];
-    for (int i = 0; i < 64; ++i) { v[i] = i < 33 ? blk[i].value : 0; bid[i] = i < 33 ? i : 0; }
-    for (int stride = 32; stride > 0; stride >>= 1)
-      for (int t = 0; t < stride; ++t)
-        if (v[t] < v[t + stride]) { v[t] = v[t + stride]; bid[t] = bid[t + stride]; }
-    const int* tg = blk[bid[0]].target;
-    if (s.begin[3] < tg[3]) { s.end[3] = tg[3]; maxlevel = 0; } else s.end[3] = s.begin[3];
-    if (s.begin[2] < tg[2]) { s.end[2] = tg[2]; maxlevel = 1; } else s.end[2] = s.begin[2];
-    if (s.begin[1] < tg[1]) { s.end[1] = tg[1]; maxlevel = 2; } else s.end[1] = s.begin[1];
-    if (s.begin[0] < tg[0]) { s.end[0] = tg[0]; maxlevel = 3; } else s.end[0] = s.begin[0];
-  }
-  s.maxlevel = maxlevel;
-  *st = s;
-}
-
-// The same on one warp (lane 0 writes the state): the 33 block maxima reduce
-// by the same tree (at each stride, position t takes t + stride's entry when
-// its value is strictly smaller), so ties resolve identically.
-__device__ __forceinline__ void strategy_finish_warp(const StrategyBlock* __restrict__ blk, int mode, double bound,
+// Reduction over the cells + begin/end/maxlevel update
+// (dataloader.cu:278-334), or loadall (:21-28) when the target is below the
+// compression bound; one warp, lane 0 writes the state.
+__device__ __forceinline__ void strategy_finish_warp(const StrategyBest* __restrict__ cells, int mode, double bound,
                                                      double target, const double* __restrict__ range,
                                                      StrategyState* __restrict__ st) {
   const int lane = threadIdx.x & 31;
   bool use_search;
   uint64_t target_cost;
   strategy_setup(mode, bound, target, range, &use_search, &target_cost);
-  int winner = 0;
+  int tg[4] = {32, 32, 32, 32};
   if (use_search) {
-    unsigned long long v = blk[lane].value;
-    int bid = lane;
-    const unsigned long long w32 = lane == 0 ? blk[32].value : 0ull;
-    if (v < w32) { v = w32; bid = 32; }
-    for (int stride = 16; stride > 0; stride >>= 1) {
-      const unsigned long long w = __shfl_down_sync(0xffffffffu, v, stride);
-      const int wb = __shfl_down_sync(0xffffffffu, bid, stride);
-      if (lane < stride && v < w) { v = w; bid = wb; }
+    unsigned long long best = 0;
+    unsigned bkey = 0;
+    for (int i = lane; i < kStrategyCells; i += 32) {
+      const StrategyBest c = cells[i];
+      if (strategy_better(c.value, c.key, best, bkey)) { best = c.value; bkey = c.key; }
     }
-    winner = __shfl_sync(0xffffffffu, bid, 0);
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+      const unsigned long long ov = __shfl_xor_sync(0xffffffffu, best, d);
+      const unsigned ok = __shfl_xor_sync(0xffffffffu, bkey, d);
+      if (strategy_better(ov, ok, best, bkey)) { best = ov; bkey = ok; }
+    }
+    if (best > 0) {  // otherwise every block reports its initial {32, 32, 32, 32}
+      const int b0 = (int)strategy_brev(63u - ((bkey >> 16) & 63u), 6);
+      const int t = (int)strategy_brev(1023u - ((bkey >> 6) & 1023u), 10);
+      const int k = 63 - (int)(bkey & 63u);
+      const int pos = k * 1024 + t;
+      tg[0] = b0;
+      tg[1] = pos / (33 * 33);
+      tg[2] = (pos / 33) % 33;
+      tg[3] = pos % 33;
+    }
   }
   if (lane != 0) return;
   StrategyState s = *st;
@@ -156,7 +171,6 @@ __device__ __forceinline__ void strategy_finish_warp(const StrategyBlock* __rest
     for (int i = 0; i < 4; ++i) s.end[i] = 32;
     maxlevel = s.begin[0] < 32 ? 3 : s.begin[1] < 32 ? 2 : s.begin[2] < 32 ? 1 : s.begin[3] < 32 ? 0 : 4;
   } else {
-    const int* tg = blk[winner].target;
     if (s.begin[3] < tg[3]) { s.end[3] = tg[3]; maxlevel = 0; } else s.end[3] = s.begin[3];
     if (s.begin[2] < tg[2]) { s.end[2] = tg[2]; maxlevel = 1; } else s.end[2] = s.begin[2];
     if (s.begin[1] < tg[1]) { s.end[1] = tg[1]; maxlevel = 2; } else s.end[1] = s.begin[1];
@@ -164,6 +178,12 @@ __device__ __forceinline__ void strategy_finish_warp(const StrategyBlock* __rest
   }
   s.maxlevel = maxlevel;
   *st = s;
+}
+
+__global__ void strategy_finish_kernel(const StrategyBest* __restrict__ cells, int mode, double bound,
+                                       double target, const double* __restrict__ range,
+                                       StrategyState* __restrict__ st) {
+  strategy_finish_warp(cells, mode, bound, target, range, st);
 }
 
 }  // namespace prism_b200
