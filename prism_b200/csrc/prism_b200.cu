@@ -470,11 +470,7 @@ static int launch_encode(prism_handle* h, const uint8_t* planes, const Geometry&
   CK(cudaMemsetAsync(&s->ticket, 0, sizeof(unsigned long long), st));
   CK(cudaMemsetAsync(&s->error_flag, 0, sizeof(int), st));
   size_t smem = sizeof(EncodeShared);
-  static bool attr_set = false;
-  if (!attr_set) {
-    CK(cudaFuncSetAttribute(zbpc_encode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr_set = true;
-  }
+  CK(smem_limit<zbpc_encode_kernel>((int)smem));
   int blocks = (int)std::min<int64_t>(g.chunks, (int64_t)h->sm_count * 4);
   prof_begin(h, kStEncode, st);
   zbpc_encode_kernel<<<blocks, kZThreads, smem, st>>>(planes, g, stream, h->status.as<unsigned long long>(),
@@ -515,11 +511,7 @@ static int launch_decode(prism_handle* h, const uint8_t* stream, uint64_t stream
     CK(cudaMemsetAsync(err, 0, sizeof(int), st));
   }
   size_t smem = sizeof(DecodeShared);
-  static bool attr_set = false;
-  if (!attr_set) {
-    CK(cudaFuncSetAttribute(zbpc_decode_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr_set = true;
-  }
+  CK(smem_limit<zbpc_decode_kernel>((int)smem));
   int blocks = (int)std::min<int64_t>(g.chunks, (int64_t)h->sm_count * 8);
   zbpc_decode_kernel<<<blocks, kZThreads, smem, st>>>(stream, stream_bytes, offs, g, planes, dbegin, dend, err);
   prof_end(h, kStDecode, st);

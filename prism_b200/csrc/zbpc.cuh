@@ -431,23 +431,28 @@ struct DecodeShared {
 // Copy n <= kChunk bytes from an arbitrarily aligned global address into
 // shared memory with aligned 32-bit loads; no byte past src + n - 1's word is
 // read.  A thread's words are w = t + k * kZThreads (k < 8); every load is
-// issued before the first store, so a chunk costs one load latency.
+// issued before the first store, so a chunk costs one load latency.  Each
+// source word is loaded once: the word after w is the next lane's (lane 31
+// loads it itself).
 __device__ __forceinline__ void copy_in(uint8_t* dst, const uint8_t* src, int n) {
   constexpr int kWords = kChunk / 4 / kZThreads;
   const int shift = (int)((uintptr_t)src & 3);
   const uint32_t* a = reinterpret_cast<const uint32_t*>(src - shift);
   const int last = (shift + n - 1) >> 2;  // last source word needed
+  const int lane = threadIdx.x & 31;
   uint32_t* dw = reinterpret_cast<uint32_t*>(dst);
   uint32_t lo[kWords], hi[kWords];
 #pragma unroll
   for (int k = 0; k < kWords; ++k) {
     const int w = threadIdx.x + k * kZThreads;
-    lo[k] = 4 * w < n ? __ldg(a + w) : 0u;
-    hi[k] = (4 * w < n && w + 1 <= last) ? __ldg(a + w + 1) : 0u;
+    lo[k] = w <= last ? __ldg(a + w) : 0u;
+    hi[k] = (lane == 31 && w + 1 <= last) ? __ldg(a + w + 1) : 0u;
   }
 #pragma unroll
   for (int k = 0; k < kWords; ++k) {
     const int w = threadIdx.x + k * kZThreads;
+    const uint32_t next = __shfl_down_sync(0xffffffffu, lo[k], 1);
+    if (lane != 31) hi[k] = next;
     if (4 * w < n) dw[w] = shift ? __funnelshift_r(lo[k], hi[k], 8 * shift) : lo[k];
   }
 }
