@@ -900,7 +900,7 @@ static int progressive_step_t(prism_prog* p, double target, const T* prev, T* va
   // it advances the object's device state in place
   const uint64_t* csbp = reinterpret_cast<const uint64_t*>(tr + 16);
   prof_begin(h, kStStrategy, st);
-  strategy_scan_kernel<<<dim3(kStrategyRounds, 33), 256, 0, st>>>(csbp, p->mode, p->bound, target, range, s->sblk);
+  strategy_scan_kernel<<<dim3(kStrategyGroups, 33), 256, 0, st>>>(csbp, p->mode, p->bound, target, range, s->sblk);
   // the strategy's plane ranges, then the parameters with its maxlevel
   prog_plan_kernel<T><<<1, 32, 0, st>>>(s->sblk, p->mode, p->bound, target, range, ds,
                                         alpha_of(p->mode == 1 ? p->bound : 0.0), tr,
@@ -1196,7 +1196,7 @@ int prism_find_strategy(prism_handle* h, const uint64_t comp_size_bp[128], doubl
   CK(cudaMemcpyAsync(&s->sstate, &tmp, sizeof(tmp), cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(h->part.p, comp_size_bp, 1024, cudaMemcpyHostToDevice, st));
   set_double_kernel<<<1, 1, 0, st>>>(&s->range, 1.0);
-  strategy_scan_kernel<<<dim3(kStrategyRounds, 33), 256, 0, st>>>(h->part.as<uint64_t>(), 0, eb, target_error,
+  strategy_scan_kernel<<<dim3(kStrategyGroups, 33), 256, 0, st>>>(h->part.as<uint64_t>(), 0, eb, target_error,
                                                                   &s->range, s->sblk);
   strategy_finish_kernel<<<1, 32, 0, st>>>(s->sblk, 0, eb, target_error, &s->range, &s->sstate);
   CK(cudaGetLastError());

@@ -6,9 +6,9 @@
 // 1024 threads; its per-thread scan (strict >), per-block tree reduction
 // (strict <, left kept) and cross-block tree reduction define which of
 // several equal-valued choices wins.  That choice is restated below as a
-// total order on the candidates, so the scan runs as 1188 small CTAs (one
-// per scan round and b0, filling the GPU) and a one-warp reduction instead
-// of 33 CTAs and the reference's spin barrier.
+// total order on the candidates, so the scan runs as 297 CTAs (one per b0
+// and group of scan rounds, filling the GPU) and a one-warp reduction
+// instead of 33 CTAs and the reference's spin barrier.
 #pragma once
 #include <stdint.h>
 
@@ -56,9 +56,13 @@ __device__ __forceinline__ void strategy_setup(int mode, double bound, double ta
 // candidate of largest value (> 0, within the cost) with ties broken by
 // bit-reversed b0, then bit-reversed t, then k.  That order is packed into
 // `key` (larger wins), which lets any reduction order find it: here one CTA
-// per (k, b0), 1188 in all, and a final warp.
+// per b0 and group of four rounds k (297 CTAs of 256 threads, 16 candidates a
+// thread), and a final warp over the 297 CTA results.
 constexpr int kStrategyRounds = (33 * 33 * 33 + 1023) / 1024;  // 36
-constexpr int kStrategyCells = kStrategyRounds * 33;
+constexpr int kStrategyRoundsPerCta = 4;
+constexpr int kStrategyGroups = kStrategyRounds / kStrategyRoundsPerCta;  // 9
+constexpr int kStrategyCells = kStrategyGroups * 33;
+static_assert(kStrategyRounds % kStrategyRoundsPerCta == 0, "whole groups of rounds");
 
 struct StrategyBest {
   unsigned long long value;
@@ -84,7 +88,7 @@ strategy_scan_kernel(const uint64_t* __restrict__ cs, int mode, double bound, do
   __shared__ uint64_t vt[4][33];
   __shared__ unsigned long long wv[8];
   __shared__ unsigned wk[8];
-  const int tid = threadIdx.x, k = blockIdx.x, b0 = blockIdx.y;
+  const int tid = threadIdx.x, group = blockIdx.x, b0 = blockIdx.y;
   if (tid < 4 * 33) {
     int l = tid / 33, b = tid % 33;
     cost[l][b] = strategy_cost(l, b);
@@ -92,19 +96,23 @@ strategy_scan_kernel(const uint64_t* __restrict__ cs, int mode, double bound, do
     vt[l][b] = b == 0 ? top : (b == 32 ? 0 : top - cs[l * 32 + b - 1]);
   }
   __syncthreads();
-  const unsigned kb = (63u - strategy_brev((unsigned)b0, 6)) << 16 | (63u - (unsigned)k);
+  const unsigned kb = (63u - strategy_brev((unsigned)b0, 6)) << 16;
   unsigned long long best = 0;
   unsigned bkey = 0;
 #pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    const int t = q * 256 + tid, pos = k * 1024 + t;
-    if (pos < 33 * 33 * 33) {
-      const int b1 = pos / (33 * 33), b2 = (pos / 33) % 33, b3 = pos % 33;
-      const uint64_t tc = cost[0][b0] + cost[1][b1] + cost[2][b2] + cost[3][b3];
-      if (tc <= target_cost) {
-        const unsigned long long v = vt[0][b0] + vt[1][b1] + vt[2][b2] + vt[3][b3];
-        const unsigned key = kb | (1023u - strategy_brev((unsigned)t, 10)) << 6;
-        if (v > 0 && strategy_better(v, key, best, bkey)) { best = v; bkey = key; }
+  for (int r = 0; r < kStrategyRoundsPerCta; ++r) {
+    const int k = group * kStrategyRoundsPerCta + r;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int t = q * 256 + tid, pos = k * 1024 + t;
+      if (pos < 33 * 33 * 33) {
+        const int b1 = pos / (33 * 33), b2 = (pos / 33) % 33, b3 = pos % 33;
+        const uint64_t tc = cost[0][b0] + cost[1][b1] + cost[2][b2] + cost[3][b3];
+        if (tc <= target_cost) {
+          const unsigned long long v = vt[0][b0] + vt[1][b1] + vt[2][b2] + vt[3][b3];
+          const unsigned key = kb | (1023u - strategy_brev((unsigned)t, 10)) << 6 | (63u - (unsigned)k);
+          if (v > 0 && strategy_better(v, key, best, bkey)) { best = v; bkey = key; }
+        }
       }
     }
   }
@@ -124,7 +132,7 @@ strategy_scan_kernel(const uint64_t* __restrict__ cs, int mode, double bound, do
     r.value = best;
     r.key = bkey;
     r.pad = 0;
-    out[b0 * kStrategyRounds + k] = r;
+    out[b0 * kStrategyGroups + group] = r;
   }
 }
 
@@ -142,10 +150,16 @@ __device__ __forceinline__ void strategy_finish_warp(const StrategyBest* __restr
   if (use_search) {
     unsigned long long best = 0;
     unsigned bkey = 0;
-    for (int i = lane; i < kStrategyCells; i += 32) {
-      const StrategyBest c = cells[i];
-      if (strategy_better(c.value, c.key, best, bkey)) { best = c.value; bkey = c.key; }
+    constexpr int kPerLane = (kStrategyCells + 31) / 32;
+    StrategyBest c[kPerLane];
+#pragma unroll
+    for (int m = 0; m < kPerLane; ++m) {  // all loads in flight before the compares
+      const int i = lane + 32 * m;
+      c[m] = i < kStrategyCells ? cells[i] : StrategyBest{0ull, 0u, 0u};
     }
+#pragma unroll
+    for (int m = 0; m < kPerLane; ++m)
+      if (strategy_better(c[m].value, c[m].key, best, bkey)) { best = c[m].value; bkey = c[m].key; }
 #pragma unroll
     for (int d = 16; d > 0; d >>= 1) {
       const unsigned long long ov = __shfl_xor_sync(0xffffffffu, best, d);
