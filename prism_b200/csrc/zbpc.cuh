@@ -457,23 +457,77 @@ __device__ __forceinline__ void copy_in(uint8_t* dst, const uint8_t* src, int n)
   }
 }
 
-// One CTA per chunk.  begin/end (device, may be null) select the chunks of
-// host planes [begin[3-l], end[3-l]) like zbpc_decode_progressive
-// (zbpc.cu:420-423).  Corrupt chunks raise error_flag = 2.  The payload is
-// decoded from its tail: bitmap 4 B -> 32 B -> 256 B -> 2048 B (fill-forward:
-// byte i = kept byte rank(i) - 1, rank the inclusive flag count), then the
-// nonzero bytes are scattered by the zero-elimination bitmap.
+// Chunk holding byte `off` of the plane buffer (host placement: level 3's 32
+// planes first, each plane cut into 16 KiB chunks; chunk ids follow the
+// bytes).  Offsets past the buffer map past the last chunk.
+__device__ __forceinline__ int64_t chunk_of_byte(const Geometry& g, int64_t off) {
+  int64_t hb = 0, cb = 0;
+  for (int l = 3; l >= 0; --l) {
+    const int64_t span = g.hastride[l] << 5;
+    if (off < hb + span || l == 0) {
+      const int64_t rel = off - hb, p = rel / g.hastride[l];
+      return cb + p * (g.chunks_level[l] >> 5) + (rel - p * g.hastride[l]) / kChunk;
+    }
+    hb += span;
+    cb += g.chunks_level[l];
+  }
+  return 0;
+}
+
+// Grid-stride over the chunks a decode must visit.  begin/end (device, may
+// be null) select the chunks of host planes [begin[3-l], end[3-l]) like
+// zbpc_decode_progressive (zbpc.cu:420-423); then per level only one range
+// of chunk ids matters: the selected planes' chunks and the chunks holding
+// the bytes the inverse shuffle reads for those planes at their device
+// placement (which are zeroed where no selected chunk covers them).  Other
+// chunks are never read, so the walk skips them.  Corrupt chunks raise
+// error_flag = 2.  The payload is decoded from its tail: bitmap 4 B -> 32 B
+// -> 256 B -> 2048 B (fill-forward: byte i = kept byte rank(i) - 1, rank the
+// inclusive flag count), then the nonzero bytes are scattered by the
+// zero-elimination bitmap.
 __global__ void __launch_bounds__(kZThreads, 4)
 zbpc_decode_kernel(const uint8_t* __restrict__ stream, uint64_t stream_bytes, const int64_t* __restrict__ offs,
                    Geometry g, uint8_t* __restrict__ planes, const int* __restrict__ begin,
                    const int* __restrict__ end, int* __restrict__ error_flag) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   DecodeShared& sh = *reinterpret_cast<DecodeShared*>(smem_raw);
+  __shared__ int64_t range_start[4], range_len[4];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int64_t chunks = g.chunks;
   const uint16_t* sizes = reinterpret_cast<const uint16_t*>(stream + 8);
   const uint8_t* data_in = stream + 8 + 2 * chunks;
-  for (int64_t id = blockIdx.x; id < chunks; id += gridDim.x) {
+  if (tid < 4) {
+    const int l = tid;
+    int64_t s = 0, e = 0;
+    if (!begin) {
+      e = l == 0 ? chunks : 0;  // a full decode: every chunk, once
+    } else if (begin[3 - l] < end[3 - l]) {
+      const int lo = begin[3 - l], hi = end[3 - l];
+      int64_t cb = 0;
+      for (int i = 3; i > l; --i) cb += g.chunks_level[i];
+      const int64_t cpp = g.chunks_level[l] >> 5;
+      s = cb + lo * cpp;
+      e = cb + hi * cpp;
+      const int64_t a = g.daprefix[l] + (int64_t)lo * g.dstride[l], b = g.daprefix[l] + (int64_t)hi * g.dstride[l];
+      const int64_t lim = (int64_t)g.aligned_size;
+      if (a < b && a < lim) {
+        const int64_t f = chunk_of_byte(g, a), t = chunk_of_byte(g, (b < lim ? b : lim) - 1) + 1;
+        s = f < s ? f : s;
+        e = t > e ? t : e;
+      }
+      s = s < 0 ? 0 : (s > chunks ? chunks : s);
+      e = e < s ? s : (e > chunks ? chunks : e);
+    }
+    range_start[l] = s;
+    range_len[l] = e - s;
+  }
+  __syncthreads();
+  const int64_t visits = range_len[0] + range_len[1] + range_len[2] + range_len[3];
+  for (int64_t v = blockIdx.x; v < visits; v += gridDim.x) {
+    int64_t id = v;
+    int r = 0;
+    while (r < 3 && id >= range_len[r]) id -= range_len[r++];
+    id += range_start[r];
     const ChunkLoc loc = locate_chunk(g, id);
     if (begin) {
       int64_t cpp = g.chunks_level[loc.level] >> 5;
