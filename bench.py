@@ -56,7 +56,64 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-class ClockSampler:
+class NvmlClockSampler:
+    """SM clock and clock-event reasons read through NVML every 2 ms during
+    the timed region (read-only queries; the GPU's settings are untouched)."""
+
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
+               "sw_power_cap": 0x4}
+
+    def __init__(self, index):
+        import threading
+
+        import pynvml
+        self.nv = pynvml
+        pynvml.nvmlInit()
+        self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+        self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
+        self.samples = []
+        self.stop_flag = threading.Event()
+        self.thread = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        nv = self.nv
+        while not self.stop_flag.is_set():
+            try:
+                self.samples.append((float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)),
+                                     int(nv.nvmlDeviceGetCurrentClocksEventReasons(self.h))))
+            except Exception:
+                pass
+            time.sleep(0.002)
+
+    def start(self):
+        self.thread.start()
+        t0 = time.time()
+        while not self.samples and time.time() - t0 < 1.0:
+            time.sleep(0.001)
+
+    def stop(self):
+        self.stop_flag.set()
+        self.thread.join(timeout=5)
+        try:
+            self.nv.nvmlShutdown()
+        except Exception:
+            pass
+        if not self.samples:
+            return None
+        reasons = sorted(n for n, bit in self.REASONS.items() if any(r & bit for _, r in self.samples))
+        return {"sm_mhz": statistics.median(c for c, _ in self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": reasons, "samples": len(self.samples), "source": "nvml, 2 ms"}
+
+
+def ClockSampler(index):
+    """NVML sampler when the binding is usable, else nvidia-smi."""
+    try:
+        return NvmlClockSampler(index)
+    except Exception:
+        return SmiClockSampler(index)
+
+
+class SmiClockSampler:
     """nvidia-smi clocks/throttle reasons sampled during the timed region."""
 
     def __init__(self, index):
@@ -114,7 +171,7 @@ class ClockSampler:
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi"}
 
 
 def make_field(rank):
