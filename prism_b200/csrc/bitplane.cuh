@@ -193,25 +193,38 @@ inverse_bitshuffle_kernel(const uint8_t* __restrict__ planes, int32_t* __restric
   if (count > kShufCodes) count = kShufCodes;
   int lo = 0, hi = 32;
   if (begin) { lo = begin[3 - level]; hi = end[3 - level]; }
+  int32_t* dst = codes + pick4(plan.seg_start, level) + first;
+  if (lo >= hi) {  // no plane of this level selected: every code is 0 in both encodings
+    for (int idx = lane; idx < count; idx += 32) dst[idx] = 0;
+    return;
+  }
   const int nbytes = (int)(count / 8);
   const int64_t stride = pick4(g.dstride, level);
   const uint8_t* base = planes + pick4(g.daprefix, level) + first / 8;
   uint32_t (&tw)[32][33] = tile[warp];
   // a[r] = the lane's word (as loaded) of plane 31 - r
   uint32_t a[32];
+  if (count == kShufCodes) {  // every item but a level's last: one word per lane and plane
 #pragma unroll
-  for (int r = 0; r < 32; ++r) {
-    const int p = 31 - r;
-    const uint8_t* src = base + (int64_t)p * stride;
-    uint32_t v = 0;
-    if (p >= lo && p < hi) {
-      if (4 * lane + 4 <= nbytes) {
-        v = __ldg(reinterpret_cast<const uint32_t*>(src) + lane);
-      } else if (4 * lane < nbytes) {
-        for (int b = 4 * lane; b < nbytes; ++b) v |= (uint32_t)src[b] << (8 * (b & 3));
-      }
+    for (int r = 0; r < 32; ++r) {
+      const int p = 31 - r;
+      a[r] = (p >= lo && p < hi) ? __ldg(reinterpret_cast<const uint32_t*>(base + (int64_t)p * stride) + lane) : 0u;
     }
-    a[r] = v;
+  } else {
+#pragma unroll
+    for (int r = 0; r < 32; ++r) {
+      const int p = 31 - r;
+      const uint8_t* src = base + (int64_t)p * stride;
+      uint32_t v = 0;
+      if (p >= lo && p < hi) {
+        if (4 * lane + 4 <= nbytes) {
+          v = __ldg(reinterpret_cast<const uint32_t*>(src) + lane);
+        } else if (4 * lane < nbytes) {
+          for (int b = 4 * lane; b < nbytes; ++b) v |= (uint32_t)src[b] << (8 * (b & 3));
+        }
+      }
+      a[r] = v;
+    }
   }
   bit_transpose32(a);
   // a[k] = transformed code 32 lane + plane_bit_code(k); out through the tile
@@ -219,7 +232,6 @@ inverse_bitshuffle_kernel(const uint8_t* __restrict__ planes, int32_t* __restric
 #pragma unroll
   for (int k = 0; k < 32; ++k) tw[lane][plane_bit_code(k)] = a[k];
   __syncwarp();
-  int32_t* dst = codes + pick4(plan.seg_start, level) + first;
 #pragma unroll 8
   for (int it = 0; it < 32; ++it) {
     const int idx = it * 32 + lane;
