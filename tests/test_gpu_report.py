@@ -87,3 +87,28 @@ def test_cli_roundtrip_with_report(env, tmp_path):
     dec = np.fromfile(str(src) + ".prisma.out", dtype=np.float32).reshape(data.shape)
     got = P.Compressor(ctx).decompress_pipeline(torch.from_numpy(cont).cuda()).cpu().numpy()
     assert np.array_equal(dec, got)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_extrema_on_unaligned_slices(env, dtype):
+    """prism_extrema on slices that start off a 16-byte boundary, with lengths
+    of 1 to the whole buffer: the range is max - min in double, with the
+    extreme values placed near the start and near the end."""
+    import ctypes as C
+    torch, P = env
+    h = P.Handle()
+    rng = np.random.default_rng(5)
+    base = rng.standard_normal((1 << 20) + 7).astype(dtype)
+    base[1] = 50.0     # in the head of an offset-1 slice
+    base[-2] = -70.0   # in the tail
+    d = torch.from_numpy(base).cuda()
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    for off in (0, 1, 2, 3):
+        for length in (1, 3, 17, base.size - off - 1, base.size - off):
+            sl = d[off:off + length]
+            rng_out = C.c_double()
+            h.check(P.lib().prism_extrema(h.ptr, C.c_void_p(sl.data_ptr()), base.itemsize, length,
+                                          C.byref(rng_out), st), "prism_extrema")
+            host = base[off:off + length]
+            want = float(host.max()) - float(host.min())
+            assert rng_out.value == want, (off, length, rng_out.value, want)
