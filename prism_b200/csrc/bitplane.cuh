@@ -154,6 +154,11 @@ __device__ __forceinline__ void shuffle_item(uint32_t (&tw)[32][33], const int32
   const int nbytes = (int)(count / 8);
   const int64_t stride = pick4(g.dstride, level);
   uint8_t* base = planes + pick4(g.daprefix, level) + first / 8;
+  if (count == kShufCodes) {  // every item but a level's last: one word per lane and plane
+#pragma unroll
+    for (int r = 0; r < 32; ++r) reinterpret_cast<uint32_t*>(base + (int64_t)(31 - r) * stride)[lane] = a[r];
+    return;
+  }
 #pragma unroll
   for (int r = 0; r < 32; ++r) {
     uint8_t* dst = base + (int64_t)(31 - r) * stride;
