@@ -463,6 +463,8 @@ def run_prism(args, world, rank, local):
     # free the single-field buffers before the batch and serving parts
     del d_in, d_cont, values, d_cont2, comp, h
     torch.cuda.empty_cache()
+    single = None if args.no_fields else run_fields(torch, P, args)
+    torch.cuda.empty_cache()
     batched = None if args.no_batch else run_batched(torch, P, args)
     torch.cuda.empty_cache()
     serving = None if args.no_serve else run_serving(torch, P, args)
@@ -485,7 +487,7 @@ def run_prism(args, world, rank, local):
                                                (csz + len(TARGETS) * field_bytes) / pcie["d2h"])},
         "roofline": roofline, "stages": stages, "cpu_baseline": cpu, "gpu_launches": launches,
         "clocks": clk,
-        "batched": batched, "serving": serving,
+        "fields": single, "batched": batched, "serving": serving,
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -544,6 +546,66 @@ def run_batched(torch, P, args):
             "batched_ms": batch_ms, "per_field_ms": plain_ms, "speedup": plain_ms / batch_ms,
             "identical_containers": identical, "runs": reps, "plan_s": plan_s, "schedule": sch,
             "data": "synthetic, generated on the device"}
+
+
+# ---------------------------------------------------------------- single fields
+def run_fields(torch, P, args):
+    """The other single-field configurations, device-resident: config 0
+    (128^3 float32 sinusoid sum, REL 1e-4; 8 MB, inside L2 and launch-bound)
+    and config 2 (1024^3 float32 piecewise-smooth Voronoi field with 30% zero
+    cells and 0.1% spikes of 1e3, ABS 1e-3; 4.3 GB).  Compress and decompress
+    through the C ABI into preallocated buffers, CUDA events around a few
+    calls (each call ends with its own stream synchronisation, as a caller's
+    does); fraction of the measured copy bandwidth from the algorithmic bytes
+    (field + container)."""
+    from prism_b200 import fields
+    peak, peak_kind = measured_peak()
+    h = P.Handle()
+    res = {}
+    cases = [("c0 128x128x128 f32 sinusoids REL 1e-4", (128, 128, 128), fields.device_sinusoid, P.REL, 1e-4, 0, 20),
+             ("c2 1024x1024x1024 f32 Voronoi (30% zero cells, 0.1% spikes) ABS 1e-3", (1024, 1024, 1024),
+              fields.device_voronoi, P.ABS, 1e-3, 2, 3)]
+    for name, (nx, ny, nz), gen, mode, bound, seed, reps in cases:
+        d = gen((nz, ny, nx), np.float32, seed).contiguous()
+        comp = P.Compressor(P.Context(nx, ny, nz, np.dtype(np.float32), mode, bound, False))
+        buf = torch.empty(comp.max_container_size(), dtype=torch.uint8, device="cuda")
+        rec = torch.empty_like(d)
+        cont = comp.compress_pipeline(d, buf)  # warm-up: workspace, auto-tune windows
+        comp.decompress_pipeline(cont, rec)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            cont = comp.compress_pipeline(d, buf)
+        e1.record()
+        e1.synchronize()
+        cms = e0.elapsed_time(e1) / reps
+        e0.record()
+        for _ in range(reps):
+            comp.decompress_pipeline(cont, rec)
+        e1.record()
+        e1.synchronize()
+        dms = e0.elapsed_time(e1) / reps
+        nbytes, cbytes = d.numel() * 4, int(cont.numel())
+        st = h.statistics(d, rec)
+        lo_v, hi_v = float(d.min().item()), float(d.max().item())
+        eb = bound if mode == P.ABS else bound * (hi_v - lo_v)
+        # the bound holds in exact arithmetic; the float32 roundings of the
+        # residual, the quantisation code and the reconstruction add a few ulp
+        # at the largest |x| (the large-field test allows 8 eps |x|max)
+        allowance = 8.0 * float(np.finfo(np.float32).eps) * max(abs(lo_v), abs(hi_v))
+        res[name] = {"compress_GBps": nbytes / cms / 1e6, "decompress_GBps": nbytes / dms / 1e6,
+                     "compress_ms": cms, "decompress_ms": dms,
+                     "compress_hbm_frac": (nbytes + cbytes) / cms / 1e6 / peak,
+                     "decompress_hbm_frac": (nbytes + cbytes) / dms / 1e6 / peak,
+                     "compression_ratio": nbytes / cbytes, "max_err": st["max_err"], "bound": eb,
+                     "value_range": [lo_v, hi_v], "float_rounding_allowance": allowance,
+                     "calls": reps, "peak_kind": f"{peak_kind} copy bandwidth",
+                     "data": "synthetic, generated on the device"}
+        del d, comp, buf, rec, cont
+        torch.cuda.empty_cache()
+    h.close()
+    return res
 
 
 # ---------------------------------------------------------------- serving
@@ -646,6 +708,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="prism", choices=["prism", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-fields", action="store_true", help="skip the config 0 and config 2 single fields")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-compression measurement")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving measurement")
     args = ap.parse_args()
