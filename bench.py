@@ -550,10 +550,10 @@ def run_batched(torch, P, args):
 
 # ---------------------------------------------------------------- single fields
 def run_fields(torch, P, args):
-    """The other single-field configurations, device-resident: config 0
-    (128^3 float32 sinusoid sum, REL 1e-4; 8 MB, inside L2 and launch-bound)
-    and config 2 (1024^3 float32 piecewise-smooth Voronoi field with 30% zero
-    cells and 0.1% spikes of 1e3, ABS 1e-3; 4.3 GB).  Compress and decompress
+    """Two more single fields, device-resident: a 128^3 float32 sinusoid sum
+    at REL 1e-4 (8 MB, inside L2 and launch-bound) and a 1024^3 float32
+    piecewise-smooth Voronoi field with 30% zero cells and 0.1% spikes of
+    1e3 at ABS 1e-3 (4.3 GB).  Compress and decompress
     through the C ABI into preallocated buffers, CUDA events around a few
     calls (each call ends with its own stream synchronisation, as a caller's
     does); fraction of the measured copy bandwidth from the algorithmic bytes
@@ -562,8 +562,8 @@ def run_fields(torch, P, args):
     peak, peak_kind = measured_peak()
     h = P.Handle()
     res = {}
-    cases = [("c0 128x128x128 f32 sinusoids REL 1e-4", (128, 128, 128), fields.device_sinusoid, P.REL, 1e-4, 0, 20),
-             ("c2 1024x1024x1024 f32 Voronoi (30% zero cells, 0.1% spikes) ABS 1e-3", (1024, 1024, 1024),
+    cases = [("128x128x128 f32 sinusoids REL 1e-4", (128, 128, 128), fields.device_sinusoid, P.REL, 1e-4, 0, 20),
+             ("1024x1024x1024 f32 Voronoi (30% zero cells, 0.1% spikes) ABS 1e-3", (1024, 1024, 1024),
               fields.device_voronoi, P.ABS, 1e-3, 2, 3)]
     for name, (nx, ny, nz), gen, mode, bound, seed, reps in cases:
         d = gen((nz, ny, nx), np.float32, seed).contiguous()
@@ -708,7 +708,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="prism", choices=["prism", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
-    ap.add_argument("--no-fields", action="store_true", help="skip the config 0 and config 2 single fields")
+    ap.add_argument("--no-fields", action="store_true", help="skip the 128^3 and 1024^3 single-field measurements")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-compression measurement")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving measurement")
     args = ap.parse_args()

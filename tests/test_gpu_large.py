@@ -1,4 +1,4 @@
-"""Config 2 scale: a 1024^3 float32 (4 GiB) piecewise-smooth field with zero
+"""A 1024^3 float32 (4 GiB) piecewise-smooth field with zero
 cells and 0.1% spikes at ABS 1e-3.  The oracle cannot run at this size in
 seconds, so the checks are size-independent properties: every value within
 the bound after a round trip, deterministic bytes, plane sizes consistent

@@ -157,8 +157,8 @@ def test_compress_is_deterministic(env):
     assert a == b
 
 
-def test_config0_matches_reference(env):
-    """Config 0 (128^3 float sinusoids, REL 1e-4): container and round trip
+def test_sinusoids_128_matches_reference(env):
+    """128^3 float sinusoids at REL 1e-4: container and round trip
     equal the reference build's."""
     torch, P, h = env
     name = "c0"
