@@ -1173,8 +1173,15 @@ __device__ __forceinline__ void compress_tile(CompressSmem<T>& sm, const T* __re
   }
 }
 
+// CTAs per SM the compiler must leave room for: a float interior tile's
+// shared memory (window + codes, 36 KB) admits six on an SM when its registers
+// do; double tiles (55 KB) and edge tiles are held to fewer by shared memory
+// and their runtime limits.
 template <class T, int PART>
-__global__ void __launch_bounds__(kPredThreads, 3)
+constexpr int predict_min_ctas() { return sizeof(T) == 4 && PART == 0 ? 6 : 3; }
+
+template <class T, int PART>
+__global__ void __launch_bounds__(kPredThreads, predict_min_ctas<T, PART>())
 predict_compress_kernel(const T* __restrict__ data, Geometry g, const PredParams<T>* __restrict__ pp,
                         T* __restrict__ anchors, int32_t* __restrict__ qc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
