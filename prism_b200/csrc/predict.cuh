@@ -1195,8 +1195,13 @@ predict_compress_kernel(const T* __restrict__ data, Geometry g, const PredParams
 // :2177-2207); PROG adds the previous values (interpolation_progressive_reverse
 // :2209-2239, shmem2global_data_progressive :1123-1147).  All codes the tile
 // can use are fetched up front with asynchronous copies.
+// a float interior tile's 23 KB of shared memory leaves room for seven
+// CTAs on an SM when its registers do; a double one (43 KB) for five
+template <class T, int PART>
+constexpr int reconstruct_min_ctas() { return PART == 0 ? (sizeof(T) == 4 ? 7 : 5) : 3; }
+
 template <class T, bool PROG, int PART>
-__global__ void __launch_bounds__(kPredThreads, PART == 0 ? 5 : 3)
+__global__ void __launch_bounds__(kPredThreads, reconstruct_min_ctas<T, PART>())
 reconstruct_kernel(const int32_t* __restrict__ qc, const T* __restrict__ anchors, Geometry g,
                    const PredParams<T>* __restrict__ pp, const T* old, T* out) {
   constexpr bool EDGE = PART == 1;
