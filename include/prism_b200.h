@@ -162,6 +162,27 @@ int prism_inverse_bitshuffle(prism_handle* h, const uint8_t* d_planes, uint32_t 
 int prism_lossless_encode(prism_handle* h, const uint8_t* d_planes, uint32_t nx, uint32_t ny,
                           uint32_t nz, uint8_t* d_stream, uint64_t capacity, uint64_t* size_out,
                           uint64_t comp_size_bp[128], void* stream);
+/* Self-test of the failure detection in the encoder's look-back (no
+ * counterpart in the reference, whose decoupled look-back in zbpc_encode,
+ * src/encoder/zbpc.cu:113-153, spins without a limit).  Runs the kernels of
+ * prism_lossless_encode with the chunk tickets starting at 1, so chunk 0 never
+ * publishes its size and every wait that reaches it gives up after
+ * `spin_limit` polls (about 64 ns apart).  Returns PRISM_ERR_TIMEOUT when the
+ * bounded wait works; the stream bytes it leaves are meaningless.  The handle
+ * stays usable.  Needs a field of at least two chunks. */
+int prism_lossless_wait_selftest(prism_handle* h, const uint8_t* d_planes, uint32_t nx, uint32_t ny,
+                                 uint32_t nz, uint8_t* d_stream, uint64_t capacity, long long spin_limit,
+                                 void* stream);
+/* Number of level-0 codes whose bits the reference's last bit-plane shuffle
+ * block does not carry for these dimensions (src/predictor/bitplane.cu:180-181,
+ * 200-260): on some shapes the block stops short of the end of the code space
+ * (trailing codes decode as 0), and on many small shapes its zero words past
+ * the end of the last level-0 plane land on the first bytes of the next
+ * planes (leading level-0 codes lose their low bits).  The container bytes
+ * stay identical to the reference's, so the points of these codes are
+ * reconstructed from a wrong code and may miss the bound.  0 for shapes
+ * without the effect.  Geometry only; no device work. */
+uint64_t prism_lost_codes(uint32_t nx, uint32_t ny, uint32_t nz);
 /* Lossless stream -> planes.  With begin/end (host, both or neither), only
  * the chunks of planes [begin[3-l], end[3-l]) of each level are decoded; of
  * the other planes, the bytes that the inverse shuffle of the selected planes

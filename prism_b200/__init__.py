@@ -75,6 +75,9 @@ def lib():
         l.prism_lossless_decode.argtypes = [vp, vp, u32, u32, u32, vp, vp, vp, vp]
         l.prism_find_strategy.argtypes = [vp, vp, dbl, dbl, vp, vp, vp, vp]
         l.prism_lossless_encode_static.argtypes = [vp, u32, u32, u32, vp, u64, C.POINTER(u64), vp, vp]
+        l.prism_lossless_wait_selftest.argtypes = [vp, vp, u32, u32, u32, vp, u64, C.c_longlong, vp]
+        l.prism_lost_codes.argtypes = [u32, u32, u32]
+        l.prism_lost_codes.restype = u64
         l.prism_batch_create.argtypes = [vp, i32, i32, C.POINTER(vp)]
         l.prism_batch_compress.argtypes = [vp, vp, vp, vp]
         l.prism_batch_schedule.argtypes = [vp, vp, vp, vp, vp]
@@ -115,8 +118,16 @@ EXPORTED = [
     "prism_batch_destroy", "prism_server_create", "prism_server_add_field", "prism_server_submit",
     "prism_server_wait", "prism_server_stats_get", "prism_server_destroy", "prism_statistics", "prism_server_poll",
     "prism_file_save", "prism_file_open", "prism_file_step", "prism_file_info", "prism_file_close",
-    "prism_progressive_step_into", "prism_profile_stages",
+    "prism_progressive_step_into", "prism_profile_stages", "prism_lossless_wait_selftest", "prism_lost_codes",
 ]
+
+
+def lost_codes(nx, ny, nz):
+    """Level-0 codes whose bits the reference's last shuffle block does not
+    carry for these dimensions (the container keeps the reference's bytes, so
+    their points may miss the bound); 0 for shapes without the effect.
+    Geometry only."""
+    return int(lib().prism_lost_codes(nx, ny, nz))
 
 STAGES = ["extrema", "autotune", "predict", "shuffle", "encode", "trailer", "strategy", "decode",
           "inverse_shuffle", "reconstruct"]

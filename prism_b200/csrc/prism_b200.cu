@@ -463,11 +463,16 @@ static int launch_inverse(prism_handle* h, const uint8_t* planes, const Geometry
   return PRISM_OK;
 }
 
+// first_ticket > 0 leaves the chunks before it unencoded, so the first
+// encoded chunk's look-back never sees its predecessor published: used only by
+// the self-test of the bounded wait (prism_lossless_wait_selftest).
 static int launch_encode(prism_handle* h, const uint8_t* planes, const Geometry& g, uint8_t* stream,
-                         cudaStream_t st) {
+                         cudaStream_t st, int first_ticket = 0, long long spin_limit = (long long)1 << 22) {
   Small* s = small(h);
   CK(cudaMemsetAsync(h->status.p, 0, (size_t)g.chunks * sizeof(unsigned long long), st));
   CK(cudaMemsetAsync(&s->ticket, 0, sizeof(unsigned long long), st));
+  // little-endian: the low byte alone makes the 64-bit ticket counter equal to first_ticket
+  if (first_ticket > 0) CK(cudaMemsetAsync(&s->ticket, first_ticket, 1, st));
   CK(cudaMemsetAsync(&s->error_flag, 0, sizeof(int), st));
   size_t smem = sizeof(EncodeShared);
   CK(smem_limit<zbpc_encode_kernel>((int)smem));
@@ -475,7 +480,7 @@ static int launch_encode(prism_handle* h, const uint8_t* planes, const Geometry&
   prof_begin(h, kStEncode, st);
   zbpc_encode_kernel<<<blocks, kZThreads, smem, st>>>(planes, g, stream, h->status.as<unsigned long long>(),
                                                       &s->ticket, s->csbp, &s->lossless_size, &s->error_flag,
-                                                      (long long)1 << 22);
+                                                      spin_limit);
   zbpc_finish_kernel<<<1, 32, 0, st>>>(stream, g, &s->lossless_size, &s->padded_size);
   prof_end(h, kStEncode, st);
   h->launches += 2;
@@ -1165,6 +1170,76 @@ int prism_lossless_encode(prism_handle* h, const uint8_t* d_planes, uint32_t nx,
   if (rc) return rc;
   *size_out = h->host->padded_size;
   return PRISM_OK;
+}
+
+int prism_lossless_wait_selftest(prism_handle* h, const uint8_t* d_planes, uint32_t nx, uint32_t ny, uint32_t nz,
+                                 uint8_t* d_stream, uint64_t capacity, long long spin_limit, void* stream) {
+  if (!h || !d_planes || !d_stream || !dims_ok(nx, ny, nz) || spin_limit < 1) return PRISM_ERR_ARG;
+  Geometry g;
+  make_geometry(nx, ny, nz, 4, &g);
+  if (g.chunks < 2) return fail(h, PRISM_ERR_ARG, "the self-test needs at least two chunks");
+  if (capacity < 8 + 2 * (uint64_t)g.chunks + g.aligned_size + 8) return fail(h, PRISM_ERR_ARG, "capacity");
+  int rc = ensure_common(h, g);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  rc = launch_encode(h, d_planes, g, d_stream, st, 1, spin_limit);
+  if (rc) return rc;
+  return finish(h, st);
+}
+
+// Level-0 codes whose bits the reference's last shuffle block does not carry
+// (bitplane.cu:180-181, 200-260, 379-380).  The block starts at device code
+// position `start`; thread t handles positions start + base + t while
+// base + t < res(t), res = tail for t > 0 and tail + align for thread 0
+// (tail = n mod 16384, or 16384), and thread t writes the transposed word of
+// position start + base + wp, wp = ((t & 63) << 3) + (t >> 6), when wp < res(t).
+//  * Real codes from the 8-code group holding position start + tail on are
+//    not transposed in full (lanes at or past tail write nothing, thread 0
+//    alone goes further and writes only the four planes of its own word) and
+//    the inverse does not decode the ones past tail.
+//  * Positions past the end of the code space read zeros; where such a
+//    position lies past its level-0 plane (byte idx / 8 >= the plane stride)
+//    its zero bytes land on byte idx / 8 - stride of the next planes, i.e. on
+//    the bits of level-0 codes 8b..8b+7 — when the last block's writes land
+//    after the first block's (as the reference's launch orders them).
+// The union of both sets, counted per level-0 code.
+static int64_t lost_codes(const Geometry& g) {
+  const int64_t start = (g.sh_grid - 1) * (int64_t)kChunk;
+  int64_t tail = (int64_t)(g.n % kChunk);
+  if (tail == 0) tail = kChunk;
+  const int64_t count0 = (int64_t)(g.n - g.grid[0]), base0 = g.dprefix[0], st = g.dstride[0];
+  const int64_t code_end = base0 + count0;
+  std::vector<uint8_t> lost((size_t)count0, 0);
+  // never transposed in full: from the 8-code group that holds position
+  // start + tail on (the lanes of that group at or past tail write nothing,
+  // and their words carry planes of the whole group; thread 0's extra
+  // positions keep only the four planes of its own word)
+  for (int64_t p = std::max(start + (tail & ~(int64_t)7), base0); p < code_end; ++p) lost[(size_t)(p - base0)] = 1;
+  // zero words past the plane
+  if (last_block_lands_last(g)) {
+    const int64_t ares = (tail + 511) / 512 * 512, ares0 = (tail + g.align_dev + 511) / 512 * 512;
+    auto mark = [&](int64_t p) {
+      if (p < code_end) return;
+      const int64_t idx = p - base0, b = (idx >> 3) - st;
+      if (idx < 0 || b < 0) return;
+      for (int64_t c = 8 * b; c < 8 * b + 8 && c < count0; ++c) lost[(size_t)c] = 1;
+    };
+    for (int64_t base = 0; base < std::max(ares, ares0); base += 512) {
+      if (base < ares)
+        for (int64_t w = 1; w < 512 && w < tail; ++w) mark(start + base + w);
+      mark(start + base);
+    }
+  }
+  int64_t cnt = 0;
+  for (uint8_t v : lost) cnt += v;
+  return cnt;
+}
+
+uint64_t prism_lost_codes(uint32_t nx, uint32_t ny, uint32_t nz) {
+  if (!dims_ok(nx, ny, nz)) return 0;
+  Geometry g;
+  make_geometry(nx, ny, nz, 4, &g);
+  return (uint64_t)lost_codes(g);
 }
 
 int prism_lossless_decode(prism_handle* h, const uint8_t* d_stream, uint32_t nx, uint32_t ny, uint32_t nz,
