@@ -133,6 +133,11 @@ void prism_progressive_close(prism_prog* p);
 /* Global range max-min in double (extrema_scan). */
 int prism_extrema(prism_handle* h, const void* d_in, int dtype_size, uint64_t n, double* range_out,
                   void* stream);
+/* Minimum and maximum of n values (host minmax_out[0], [1], converted to
+ * double): the two results of extrema_scan (include/compressor.hpp:10-31),
+ * which StatBuffer::findMinMax turns into the REL range. */
+int prism_extrema_minmax(prism_handle* h, const void* d_in, int dtype_size, uint64_t n, double minmax_out[2],
+                         void* stream);
 /* Auto-tune error sums (15 values, host) and the decisions (use_md[4], reverse[4]). */
 int prism_autotune(prism_handle* h, const void* d_in, int dtype_size, uint32_t nx, uint32_t ny,
                    uint32_t nz, double* errors_out, uint8_t flags_out[8], void* stream);

@@ -76,6 +76,7 @@ def lib():
         l.prism_find_strategy.argtypes = [vp, vp, dbl, dbl, vp, vp, vp, vp]
         l.prism_lossless_encode_static.argtypes = [vp, u32, u32, u32, vp, u64, C.POINTER(u64), vp, vp]
         l.prism_lossless_wait_selftest.argtypes = [vp, vp, u32, u32, u32, vp, u64, C.c_longlong, vp]
+        l.prism_extrema_minmax.argtypes = [vp, vp, i32, u64, vp, vp]
         l.prism_lost_codes.argtypes = [u32, u32, u32]
         l.prism_lost_codes.restype = u64
         l.prism_batch_create.argtypes = [vp, i32, i32, C.POINTER(vp)]
@@ -119,6 +120,7 @@ EXPORTED = [
     "prism_server_wait", "prism_server_stats_get", "prism_server_destroy", "prism_statistics", "prism_server_poll",
     "prism_file_save", "prism_file_open", "prism_file_step", "prism_file_info", "prism_file_close",
     "prism_progressive_step_into", "prism_profile_stages", "prism_lossless_wait_selftest", "prism_lost_codes",
+    "prism_extrema_minmax",
 ]
 
 

@@ -299,7 +299,8 @@ extrema_kernel(const T* __restrict__ in, uint64_t n, T* __restrict__ part) {
 
 // one warp folds the per-block extrema (min/max are order independent)
 template <class T>
-__global__ void extrema_final_kernel(const T* __restrict__ part, int nblocks, double* __restrict__ range) {
+__global__ void extrema_final_kernel(const T* __restrict__ part, int nblocks, double* __restrict__ range,
+                                     double* __restrict__ minmax = nullptr) {
   const int lane = threadIdx.x;
   T mn = part[0], mx = part[1];
   for (int b = lane; b < nblocks; b += 32) {
@@ -313,7 +314,13 @@ __global__ void extrema_final_kernel(const T* __restrict__ part, int nblocks, do
     mn = a < mn ? a : mn;
     mx = c > mx ? c : mx;
   }
-  if (lane == 0) *range = __dsub_rn((double)mx, (double)mn);
+  if (lane == 0) {
+    *range = __dsub_rn((double)mx, (double)mn);
+    if (minmax) {
+      minmax[0] = (double)mn;
+      minmax[1] = (double)mx;
+    }
+  }
 }
 
 }  // namespace prism_b200

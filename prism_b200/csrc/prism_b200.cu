@@ -64,6 +64,7 @@ struct Small {
   StrategyState sstate;
   StrategyBest sblk[kStrategyCells];
   double errors[16];
+  double minmax[2];
 };
 
 struct HostResult {
@@ -337,7 +338,7 @@ static int launch_extrema(prism_handle* h, const T* in, uint64_t n, cudaStream_t
   CKA(h->part.ensure(sizeof(T) * 2 * blocks));
   prof_begin(h, kStExtrema, st);
   extrema_kernel<T><<<blocks, kExtThreads, 0, st>>>(in, n, h->part.as<T>());
-  extrema_final_kernel<T><<<1, 32, 0, st>>>(h->part.as<T>(), blocks, &small(h)->range);
+  extrema_final_kernel<T><<<1, 32, 0, st>>>(h->part.as<T>(), blocks, &small(h)->range, small(h)->minmax);
   prof_end(h, kStExtrema, st);
   h->launches += 2;
   CK(cudaGetLastError());
@@ -1019,6 +1020,19 @@ int prism_extrema(prism_handle* h, const void* d_in, int dtype_size, uint64_t n,
                            : launch_extrema<double>(h, (const double*)d_in, n, st);
   if (rc) return rc;
   CK(cudaMemcpyAsync(range_out, &small(h)->range, sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return PRISM_OK;
+}
+
+int prism_extrema_minmax(prism_handle* h, const void* d_in, int dtype_size, uint64_t n, double minmax_out[2],
+                         void* stream) {
+  if (!h || !d_in || !minmax_out || n == 0 || (dtype_size != 4 && dtype_size != 8)) return PRISM_ERR_ARG;
+  CKA(h->small.ensure(sizeof(Small)));
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc = dtype_size == 4 ? launch_extrema<float>(h, (const float*)d_in, n, st)
+                           : launch_extrema<double>(h, (const double*)d_in, n, st);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(minmax_out, small(h)->minmax, 2 * sizeof(double), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   return PRISM_OK;
 }

@@ -1,130 +1,114 @@
-// C++ drop-in for the reference's prism::Compressor<T,E> pipeline
-// (include/compressor.hpp:35-83) on top of the prism_b200 C ABI.
+// The PRISM pipeline class, source-compatible with the reference's
+// prism::Compressor<T,E> and prism::StatBuffer<T> (include/compressor.hpp:
+// 10-90): same template parameters, public members and method signatures,
+// implemented over the prism_b200 C ABI (include/prism_b200.h) on the
+// sm_100a kernels.  A reference caller recompiles against these headers and
+// links libprism_b200 (and this directory's io.cpp, compressor.cpp,
+// parameters.cpp, prism.cpp).
 //
-// Buffers are device pointers owned by the caller; a Compressor owns the
-// device workspace (prism_handle).  The pipeline methods keep the reference's
-// names: compress_pipeline / decompress_pipeline /
-// decompress_progressive_pipeline.  Errors throw prism::Error instead of
-// exiting the process.
+// Differences a caller can see: failures throw prism::Error instead of ending
+// the process; the intermediate buffers qc, bp and compressed_data are sized
+// for this library's kernels (compressed_data holds the largest possible
+// container, the reference's 4n + 32 bytes can overflow); begin/end are the
+// prism_context arrays in managed memory; the stage times are CUDA-event
+// times of this library's stages.
 #pragma once
-#include <cuda_runtime.h>
-#include <stdint.h>
-
 #include <array>
-#include <stdexcept>
-#include <string>
+#include <cstddef>
 
+#include "io.hpp"
 #include "parameters.hpp"
 #include "prism_b200.h"
+#include "timer.hpp"
 
 namespace prism {
 
-struct Error : std::runtime_error {
-  int code;
-  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
-};
+// minimum and maximum of the device array data[0, len): result[0], result[1]
+template <typename T>
+void extrema_scan(T* data, size_t len, T* result);
 
 template <typename T>
+struct StatBuffer : Buffer {
+  double minVal{0.0}, maxVal{0.0}, range{1.0};
+  StatBuffer() : Buffer() {}
+  template <typename... Dim>
+  StatBuffer(prism_dtype dtype, Dim... args) : Buffer(dtype, args...) {}
+
+  // REL mode: the range max - min of the field on the device
+  double findMinMax() {
+    T result[2];
+    extrema_scan<T>(reinterpret_cast<T*>(d), len, result);
+    minVal = result[0];
+    maxVal = result[1];
+    range = maxVal - minVal;
+    return range;
+  }
+};
+
+template <typename T, typename E>
 class Compressor {
  public:
-  static_assert(sizeof(T) == 4 || sizeof(T) == 8, "float or double");
-  size_t len{0};
-  uint64_t total_compressed_size{0};
-  std::array<bool, 4> use_md{}, reverse{};
-  double time_total{0.0};  // ms, device time of the last pipeline call
+  size_t len;
+  size_t bytes_;
+  int radius;
+  int align{0};
+  int HEADERSIZE{0};  // container trailer bytes
+  double range{1.0};  // REL range read from a container's trailer
+  double time_pred{0.0}, time_bitplane{0.0}, time_encode{0.0};
+  double itime_pred{0.0}, itime_bitplane{0.0}, itime_decode{0.0}, itime_enum{0.0};
+  inBuffer* qc{nullptr};                // level-major quantisation codes
+  inBuffer* ap{nullptr};                // anchors
+  Buffer* compressed_data{nullptr};     // the container
+  Buffer* profiling_errors{nullptr};    // auto-tune error sums
+  olBuffer<T>* ol{nullptr};
+  Bitplane* bp{nullptr};                // bit planes
+  uint8_t* compressed_bp{nullptr};
+  int *begin{nullptr}, *end{nullptr};   // the prism_context plane ranges
+  size_t compressed_lossless_size{0};
+  size_t total_compressed_size{0};
+  std::array<std::array<size_t, 32>, 4> compressedSize_bp{};  // cumulative bytes per plane, [3 - level][plane]
+  size_t* compressedSize_bp_d{nullptr};                        // the same on the device
 
-  Compressor() {
-    int rc = prism_create(&h_);
-    if (rc) throw Error(rc, "prism_create failed");
-  }
-  ~Compressor() {
-    if (prog_) prism_progressive_close(prog_);
-    prism_destroy(h_);
-  }
+  Compressor() {}
+  ~Compressor();
   Compressor(const Compressor&) = delete;
   Compressor& operator=(const Compressor&) = delete;
 
-  void init(const prism_context* c) {
-    cfg_ = *c;
-    len = (size_t)c->x * c->y * c->z;
-  }
-  uint64_t max_compressed_size() const { return prism_max_container_size(cfg_.x, cfg_.y, cfg_.z, sizeof(T)); }
+  void init(prism_context* config);
+  void compute_align();
+  // input -> compressed_data (total_compressed_size bytes); the auto-tune
+  // decisions go to config->intp_param
+  void compress_pipeline(context* config, StatBuffer<T>* input, void* stream);
+  void compress_predict(context* config, StatBuffer<T>* input, void* stream);
+  void compress_merge(context* config, double input_range, void* stream);
 
-  // d_in: device field; d_out: device buffer of max_compressed_size() bytes
-  void compress_pipeline(const T* d_in, uint8_t* d_out, cudaStream_t stream) {
-    uint8_t flags[8];
-    double bound = cfg_.error_mode == REL ? cfg_.rel_eb : cfg_.eb;
-    Timer t(stream);
-    check(prism_compress(h_, d_in, sizeof(T), cfg_.x, cfg_.y, cfg_.z, cfg_.error_mode, bound,
-                         cfg_.bt == NB, d_out, max_compressed_size(), &total_compressed_size, flags, stream));
-    time_total = t.stop();
-    for (int i = 0; i < 4; ++i) { use_md[i] = flags[i]; reverse[i] = flags[4 + i]; }
-  }
+  // compressed_data (its `bytes` = the container's size) -> output
+  void decompress_pipeline(context* config, StatBuffer<T>* output, void* stream);
+  template <int init_ap>
+  void decompress_scatter(context* config, void* stream);
+  void decompress_predict(context* config, StatBuffer<T>* output, void* stream);
 
-  void decompress_pipeline(const uint8_t* d_cont, uint64_t size, T* d_out, cudaStream_t stream) {
-    double bound = cfg_.error_mode == REL ? cfg_.rel_eb : cfg_.eb;
-    Timer t(stream);
-    check(prism_decompress(h_, d_cont, size, sizeof(T), cfg_.x, cfg_.y, cfg_.z, cfg_.error_mode, bound, d_out,
-                           stream));
-    time_total = t.stop();
-  }
+  // one progressive step from the planes in [config->begin, config->end) to
+  // those targetError needs: output_new = the refinement of output_old
+  // (lastError == 0: the first step, output_old unused)
+  void decompress_progressive_pipeline(context* config, StatBuffer<T>* output_old, StatBuffer<T>* output_new,
+                                       double targetError, double lastError, void* stream);
+  void decompress_progressive_predict(context* config, StatBuffer<T>* output_old, StatBuffer<T>* output_new,
+                                      void* stream);
 
-  // One progressive step; the first call opens the resident state.  d_values
-  // is refined in place (the first step overwrites it).
-  void decompress_progressive_pipeline(const uint8_t* d_cont, uint64_t size, T* d_values, double target_error,
-                                       cudaStream_t stream) {
-    double bound = cfg_.error_mode == REL ? cfg_.rel_eb : cfg_.eb;
-    if (!prog_) check(prism_progressive_open(h_, d_cont, size, sizeof(T), cfg_.x, cfg_.y, cfg_.z, cfg_.error_mode,
-                                             bound, &prog_));
-    Timer t(stream);
-    check(prism_progressive_step(prog_, target_error, d_values, stream));
-    time_total = t.stop();
-    check(prism_progressive_state(prog_, nullptr, nullptr, nullptr, nullptr));  // device-side errors of the step
-  }
-  // The step out of place, with the reference's argument pair (output_old,
-  // output_new): d_old holds the previous step's values (nullptr on the first
-  // step) and d_new receives the refined ones.
-  void decompress_progressive_pipeline(const uint8_t* d_cont, uint64_t size, const T* d_old, T* d_new,
-                                       double target_error, cudaStream_t stream) {
-    double bound = cfg_.error_mode == REL ? cfg_.rel_eb : cfg_.eb;
-    if (!prog_) check(prism_progressive_open(h_, d_cont, size, sizeof(T), cfg_.x, cfg_.y, cfg_.z, cfg_.error_mode,
-                                             bound, &prog_));
-    Timer t(stream);
-    check(prism_progressive_step_into(prog_, target_error, d_old, d_new, stream));
-    time_total = t.stop();
-    check(prism_progressive_state(prog_, nullptr, nullptr, nullptr, nullptr));
-  }
-  void progressive_state(int begin[4], int end[4], int* maxlevel, uint64_t* loaded = nullptr) const {
-    prism_progressive_state(prog_, begin, end, maxlevel, loaded);
-  }
+  // planes selected by the last progressive step (dataloader.cu:11)
+  int maxlevel{4};
 
  private:
-  struct Timer {
-    cudaEvent_t a, b;
-    cudaStream_t s;
-    explicit Timer(cudaStream_t st) : s(st) {
-      cudaEventCreate(&a);
-      cudaEventCreate(&b);
-      cudaEventRecord(a, s);
-    }
-    double stop() {
-      float ms = 0;
-      cudaEventRecord(b, s);
-      cudaEventSynchronize(b);
-      cudaEventElapsedTime(&ms, a, b);
-      return ms;
-    }
-    ~Timer() {
-      cudaEventDestroy(a);
-      cudaEventDestroy(b);
-    }
-  };
-  void check(int rc) {
-    if (rc) throw Error(rc, std::string("prism_b200: ") + prism_last_error(h_));
-  }
   prism_handle* h_{nullptr};
-  prism_prog* prog_{nullptr};
-  prism_context cfg_{};
+  prism_context* cfg_{nullptr};
+  size_t cap_{0};  // device bytes of compressed_data
+  uint8_t flags_[8]{};
+  void check(int rc, const char* what);
+  void read_trailer(context* config, bool anchors, void* stream);
 };
+
+extern template class Compressor<float, i4>;
+extern template class Compressor<double, i4>;
 
 }  // namespace prism

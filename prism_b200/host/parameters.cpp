@@ -1,6 +1,8 @@
 // Flag parsing for the prism CLI (restates src/utils/parameters.cu:9-234).
 #include "parameters.hpp"
 
+#include <cuda_runtime.h>
+
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -58,7 +60,7 @@ static int check(prism_context* c) {
   return 0;
 }
 
-int parse_argv(prism_context* c, int argc, char** argv) {
+int prism_parse_argv(prism_context* c, int argc, char** argv) {
   if (argc == 1) usage();
   try {
     for (int i = 1; i < argc; ++i) {
@@ -129,6 +131,21 @@ int parse_argv(prism_context* c, int argc, char** argv) {
     std::cerr << "bad number in the command line: " << e.what() << std::endl;
     return 1;
   }
-  c->size = (uint64_t)c->x * c->y * c->z;
+  c->size = c->x * c->y * c->z * c->w;
+  // the progressive plane ranges (parameters.cu:161-164): managed memory, so
+  // the host reads them and callers may still clear them with cudaMemset
+  if (!c->begin && cudaMallocManaged(&c->begin, 4 * sizeof(int)) != cudaSuccess) {
+    std::cerr << "cannot allocate the plane ranges" << std::endl;
+    return 1;
+  }
+  if (!c->end && cudaMallocManaged(&c->end, 4 * sizeof(int)) != cudaSuccess) {
+    std::cerr << "cannot allocate the plane ranges" << std::endl;
+    return 1;
+  }
+  for (int i = 0; i < 4; ++i) c->begin[i] = c->end[i] = 0;
   return check(c);
+}
+
+void parse_argv(prism_context* c, int argc, char** argv) {
+  if (prism_parse_argv(c, argc, argv)) std::exit(1);
 }

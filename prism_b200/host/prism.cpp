@@ -1,138 +1,201 @@
-// CLI flows over the C++ Compressor (restates src/prism.cu:9-192 and the
-// report helpers of include/utils/analyze.hpp:5-159).
+// The PRISM flows (restates src/prism.cu:9-192 and the report helpers of
+// include/utils/analyze.hpp:5-159 of the reference) over prism::Compressor
+// and prism::StatBuffer: compress a field file into a container file,
+// decompress a container, or refine a progressive container step by step
+// through the -errors targets, with the same files, defaults and printed
+// lines.  The error statistics of --report cr run on the GPU
+// (prism_statistics) instead of host loops, and a progressive run keeps its
+// container on the device across steps instead of reloading the file.
 #include "prism.hpp"
 
 #include <cmath>
 #include <cstdio>
-#include <fstream>
 #include <iostream>
-#include <vector>
+#include <array>
+#include <memory>
 
 #include "compressor.hpp"
 
 namespace {
 
-bool read_file(const std::string& path, std::vector<char>& buf, size_t min_bytes) {
-  std::ifstream f(path, std::ios::binary | std::ios::ate);
-  if (!f) { std::cerr << "Failed to open file: " << path << std::endl; return false; }
-  size_t len = (size_t)f.tellg();
-  if (len < min_bytes) { std::cerr << "File read incomplete or corrupted: " << path << std::endl; return false; }
-  buf.resize(len);
-  f.seekg(0);
-  f.read(buf.data(), (std::streamsize)len);
-  return true;
+template <typename T, int DECOMP, int PROGRESSIVE>
+void print_result(size_t n, size_t total_compressed_size, double t_enum, double t_pred, double t_plane,
+                  double t_lossless) {
+  const double total_bytes = (double)n * sizeof(T);
+  auto gbs = [&](double ms) { return total_bytes / 1024 / 1024 / 1024 / ms * 1000; };
+  printf("\n  \033[1m%-12s %-12s %-20s\033[0m\n", "type", "time (ms)", "throughtput (GB/s)");
+  if (DECOMP) {
+    if (PROGRESSIVE) printf("  %-12s %-12f %-10.4f\n", "loadStrategy", t_enum, gbs(t_enum));
+    printf("  %-12s %-12f %-10.4f\n", "ipredict", t_pred, gbs(t_pred));
+    printf("  %-12s %-12f %-10.4f\n", "ibitplane", t_plane, gbs(t_plane));
+    printf("  %-12s %-12f %-10.4f\n", "ilossless", t_lossless, gbs(t_lossless));
+    const double total = t_pred + t_plane + t_lossless + (PROGRESSIVE ? t_enum : 0.0);
+    printf("  \033[1m%-12s\033[0m %-12f %-10.4f\n\n", "itotal", total, gbs(total));
+  } else {
+    printf("  %-12s %-12f %-10.4f\n", "predict", t_pred, gbs(t_pred));
+    printf("  %-12s %-12f %-10.4f\n", "bitplane", t_plane, gbs(t_plane));
+    printf("  %-12s %-12f %-10.4f\n", "lossless", t_lossless, gbs(t_lossless));
+    const double total = t_pred + t_plane + t_lossless;
+    printf("  \033[1m%-12s\033[0m %-12f %-10.4f\n\n", "total", total, gbs(total));
+    printf("  compression ratio: %lf\n", total_bytes / total_compressed_size);
+    printf("--------------------------------------\n");
+  }
 }
 
-bool write_file(const std::string& path, const void* p, size_t n) {
-  std::ofstream f(path, std::ios::binary);
-  if (!f) { std::cerr << "can't open file" << std::endl; return false; }
-  f.write((const char*)p, (std::streamsize)n);
-  return true;
-}
-
-// statistic (analyze.hpp:5-73) on the GPU: max error, max relative error,
-// PSNR, NRMSE of d_dat against d_ori (both on the device)
+// error statistics of a reconstruction against the original, both on the
+// device (statistic, analyze.hpp:5-73)
 template <typename T>
-void statistic(prism_handle* h, const T* d_ori, const T* d_dat, size_t n, cudaStream_t st) {
+void statistic(const T* d_ori, const T* d_dat, size_t n, void* stream) {
+  prism_handle* h = nullptr;
+  if (prism_create(&h)) return;
   double s[7];
   uint64_t idx = 0;
-  if (prism_statistics(h, d_ori, d_dat, sizeof(T), n, s, &idx, st) != PRISM_OK) {
+  if (prism_statistics(h, d_ori, d_dat, sizeof(T), n, s, &idx, stream) == PRISM_OK) {
+    printf("  Max_E  = %.15lf, idx = %d\n", s[0], (int)idx);
+    printf("  Max_RE = %G\n", s[1]);
+    printf("  PSNR = %.7lf, NRMSE = %.10G\n", s[2], s[3]);
+  } else {
     std::cerr << "statistics failed: " << prism_last_error(h) << std::endl;
-    return;
   }
-  printf("  Max_E  = %.15lf, idx = %d\n", s[0], (int)idx);
-  printf("  Max_RE = %G\n", s[1]);
-  printf("  PSNR = %.7lf, NRMSE = %.10G\n", s[2], s[3]);
+  prism_destroy(h);
 }
 
-void print_time(const char* what, size_t bytes, double ms) {
-  printf("\n  %-12s %-12s %-20s\n", "type", "time (ms)", "throughtput (GB/s)");
-  printf("  %-12s %-12f %-10.4f\n", what, ms, 1.0 * bytes / 1024 / 1024 / 1024 / ms * 1000);
+// bytes of the planes the last step selected, added to the running total
+// (calculate_accumulate_size, analyze.hpp:118-159): the per-plane size is the
+// difference of consecutive cumulative sizes, across levels at plane 0
+void accumulate_size(size_t& loaded, size_t n, int tsize, const int* begin, const int* end,
+                     const std::array<std::array<size_t, 32>, 4>& cum) {
+  const double total_bytes = (double)n * tsize;
+  size_t step = 0;
+  for (int l = 0; l < 4; ++l)
+    for (int b = begin[l]; b < end[l]; ++b) {
+      const size_t prev = b > 0 ? cum[l][b - 1] : (l > 0 ? cum[l - 1][31] : 0);
+      step += cum[l][b] - prev;
+    }
+  loaded += step;
+  printf("  Data Chunk: %zu (%lf%%)\n", step, 100.0 * step / total_bytes);
+  printf("  Total Retrieved size: %zu (%lf%%)\n", loaded, 100.0 * loaded / total_bytes);
+  printf("  Bit rate: %lf\n", 8.0 * tsize * loaded / total_bytes);
+  printf("--------------------------------------\n");
 }
 
 template <typename T>
-int run(prism_context* c) {
-  cudaStream_t st;
-  cudaStreamCreate(&st);
-  const size_t n = c->size, bytes = n * sizeof(T);
-  prism::Compressor<T> comp;
-  comp.init(c);
-  T* d_data = nullptr;
-  uint8_t* d_cont = nullptr;
-  cudaMalloc(&d_data, bytes);
-  cudaMalloc(&d_cont, comp.max_compressed_size());
-  std::vector<char> ori;
-  T* d_ori = nullptr;  // original on the device for --report cr
-  prism_handle* stat_h = nullptr;
+void compress(prism_context* c, cudaStream_t st) {
+  auto input = std::make_unique<prism::StatBuffer<T>>(c->dtype, 0, c->x, c->y, c->z);
+  input->template load_fromfile<ori_File>(c->oriFilePath);
+  input->H2D();
+  if (c->error_mode == REL) c->eb = c->rel_eb * input->findMinMax();
+  if (!c->isComp) return;
+  if (c->report_time) {  // warm up
+    prism::Compressor<T, i4> tmp;
+    tmp.init(c);
+    tmp.compress_pipeline(c, input.get(), st);
+  }
+  prism::Compressor<T, i4> cmp;
+  cmp.init(c);
+  cmp.compress_pipeline(c, input.get(), st);
+  cmp.compressed_data->unload_tofile(c->cmpFilePath, (long long)cmp.total_compressed_size,
+                                     prism::typetofile::deviceTofile);
+  if (c->report_time)
+    print_result<T, 0, 0>(cmp.len, cmp.total_compressed_size, cmp.itime_enum, cmp.time_pred, cmp.time_bitplane,
+                          cmp.time_encode);
+}
+
+template <typename T>
+void decompress(prism_context* c, cudaStream_t st) {
+  const size_t n = (size_t)c->x * c->y * c->z;
+  if (c->report_time) {  // warm up
+    prism::StatBuffer<T> out(c->dtype, 0, c->x, c->y, c->z);
+    prism::Compressor<T, i4> tmp;
+    tmp.init(c);
+    tmp.compressed_data->template load_fromfile<cmp_File>(c->cmpFilePath);
+    tmp.compressed_data->H2D();
+    tmp.decompress_pipeline(c, &out, st);
+  }
+  prism::Compressor<T, i4> dec;
+  dec.init(c);
+  dec.compressed_data->template load_fromfile<cmp_File>(c->cmpFilePath);
+  dec.compressed_data->H2D();
+  prism::StatBuffer<T> out(c->dtype, 0, c->x, c->y, c->z);
+  dec.decompress_pipeline(c, &out, st);
+  out.unload_tofile(c->decFilePath, prism::typetofile::deviceTofile);
+  if (c->report_time)
+    print_result<T, 1, 0>(n, dec.total_compressed_size, dec.itime_enum, dec.itime_pred, dec.itime_bitplane,
+                          dec.itime_decode);
   if (c->report_cr) {
-    cudaMalloc(&d_ori, bytes);
-    prism_create(&stat_h);
+    prism::StatBuffer<T> ori(c->dtype, 0, c->x, c->y, c->z);
+    ori.template load_fromfile<ori_File>(c->oriFilePath);
+    ori.H2D();
+    statistic<T>(static_cast<const T*>(ori.d), static_cast<const T*>(out.d), n, st);
   }
-  auto upload_ori = [&]() {
-    if (d_ori && !ori.empty()) cudaMemcpy(d_ori, ori.data(), bytes, cudaMemcpyHostToDevice);
-  };
-  try {
-    if (c->isComp) {
-      if (!read_file(c->oriFilePath, ori, bytes)) return 1;
-      cudaMemcpy(d_data, ori.data(), bytes, cudaMemcpyHostToDevice);
-      if (c->report_time) comp.compress_pipeline(d_data, d_cont, st);  // warm up
-      comp.compress_pipeline(d_data, d_cont, st);
-      std::vector<char> out(comp.total_compressed_size);
-      cudaMemcpy(out.data(), d_cont, out.size(), cudaMemcpyDeviceToHost);
-      if (!write_file(c->cmpFilePath, out.data(), out.size())) return 1;
-      std::cout << "compressed file written: " << c->cmpFilePath << '\n';
-      if (c->report_time) {
-        print_time("total", bytes, comp.time_total);
-        printf("\n  compression ratio: %lf\n--------------------------------------\n",
-               1.0 * bytes / comp.total_compressed_size);
-      }
-    }
-    if (c->isDecomp) {
-      std::vector<char> cont;
-      if (!read_file(c->cmpFilePath, cont, 0)) return 1;
-      cudaMemcpy(d_cont, cont.data(), cont.size(), cudaMemcpyHostToDevice);
-      if (c->report_cr && ori.empty() && !read_file(c->oriFilePath, ori, bytes)) return 1;
-      upload_ori();
-      std::vector<T> host(n);
-      if (c->compMode && !c->target_ebs.empty()) {
-        cudaMemset(d_data, 0, bytes);
-        for (size_t i = 0; i < c->target_ebs.size(); ++i) {
-          comp.decompress_progressive_pipeline(d_cont, cont.size(), d_data, c->target_ebs[i], st);
-          if (c->report_time) print_time("itotal", bytes, comp.time_total);
-          if (c->report_cr) {
-            statistic<T>(stat_h, d_ori, d_data, n, st);
-            int b[4], e[4], ml;
-            uint64_t loaded = 0;
-            comp.progressive_state(b, e, &ml, &loaded);
-            // calculate_accumulate_size (analyze.hpp:118-159)
-            printf("  Planes loaded per level: %d %d %d %d\n", e[0], e[1], e[2], e[3]);
-            printf("  Total Retrieved size: %llu (%lf%%)\n", (unsigned long long)loaded, 100.0 * loaded / bytes);
-            printf("  Bit rate: %lf\n--------------------------------------\n", sizeof(T) * 8.0 * loaded / bytes);
-          }
-        }
-      } else {
-        comp.decompress_pipeline(d_cont, cont.size(), d_data, st);
-        if (c->report_time) print_time("itotal", bytes, comp.time_total);
-      }
-      cudaMemcpy(host.data(), d_data, bytes, cudaMemcpyDeviceToHost);
-      if (!write_file(c->decFilePath, host.data(), bytes)) return 1;
-      std::cout << "decompressed file written: " << c->decFilePath << '\n';
-      if (c->report_cr && !(c->compMode && !c->target_ebs.empty())) statistic<T>(stat_h, d_ori, d_data, n, st);
-    }
-  } catch (const prism::Error& e) {
-    std::cerr << e.what() << std::endl;
-    return 2;
+}
+
+template <typename T>
+void progressive(prism_context* c, cudaStream_t st) {
+  const size_t n = (size_t)c->x * c->y * c->z;
+  std::unique_ptr<prism::StatBuffer<T>> ori;
+  if (c->report_cr) {
+    ori = std::make_unique<prism::StatBuffer<T>>(c->dtype, 0, c->x, c->y, c->z);
+    ori->template load_fromfile<ori_File>(c->oriFilePath);
+    ori->H2D();
   }
-  cudaFree(d_data);
-  cudaFree(d_cont);
-  if (d_ori) cudaFree(d_ori);
-  if (stat_h) prism_destroy(stat_h);
-  cudaStreamDestroy(st);
-  return 0;
+  prism::Compressor<T, i4> dec;
+  dec.init(c);
+  dec.compressed_data->template load_fromfile<cmp_File>(c->cmpFilePath);
+  dec.compressed_data->H2D();
+  auto cur = std::make_unique<prism::StatBuffer<T>>(c->dtype, 0, c->x, c->y, c->z);
+  auto prev = std::make_unique<prism::StatBuffer<T>>(c->dtype, 0, c->x, c->y, c->z);
+  if (c->report_time) {  // warm up, then start over from no planes
+    dec.decompress_progressive_pipeline(c, nullptr, cur.get(), c->target_ebs[0], 0, st);
+    CHECK_CUDA(cudaMemset(c->begin, 0, 4 * sizeof(int)));
+    CHECK_CUDA(cudaMemset(c->end, 0, 4 * sizeof(int)));
+  }
+  size_t loaded = dec.ap->bytes;
+  for (size_t i = 0; i < c->target_ebs.size(); ++i) {
+    std::swap(prev, cur);
+    dec.decompress_progressive_pipeline(c, prev.get(), cur.get(), c->target_ebs[i], i ? c->target_ebs[i - 1] : 0.0,
+                                        st);
+    if (c->report_time)
+      print_result<T, 1, 1>(n, dec.total_compressed_size, dec.itime_enum, dec.itime_pred, dec.itime_bitplane,
+                            dec.itime_decode);
+    if (c->report_cr) {
+      statistic<T>(static_cast<const T*>(ori->d), static_cast<const T*>(cur->d), n, st);
+      CHECK_CUDA(cudaDeviceSynchronize());
+      accumulate_size(loaded, n, (int)sizeof(T), c->begin, c->end, dec.compressedSize_bp);
+    }
+  }
+  cur->unload_tofile(c->decFilePath, prism::typetofile::deviceTofile);
+}
+
+template <typename T>
+void run(prism_context* c, cudaStream_t st) {
+  if (c->isComp) compress<T>(c, st);
+  if (c->isDecomp) {
+    if (c->compMode && !c->target_ebs.empty()) progressive<T>(c, st);
+    else decompress<T>(c, st);
+  }
 }
 
 }  // namespace
 
-int initialize(prism_context* config) {
-  return config->dtype == F4 ? run<float>(config) : run<double>(config);
+int prism_initialize(prism_context* config) {
+  cudaStream_t st;
+  if (cudaStreamCreate(&st) != cudaSuccess) {
+    std::cerr << "cannot create a CUDA stream" << std::endl;
+    return 2;
+  }
+  int rc = 0;
+  try {
+    if (config->dtype == PRISM_TYPE_DOUBLE) run<double>(config, st);
+    else run<float>(config, st);
+  } catch (const prism::Error& e) {
+    std::cerr << e.what() << std::endl;
+    rc = 2;
+  }
+  cudaStreamDestroy(st);
+  return rc;
+}
+
+void initialize(prism_context* config) {
+  if (prism_initialize(config)) std::exit(EXIT_FAILURE);
 }

@@ -1,7 +1,11 @@
-// CLI driver (the reference's include/prism.hpp:5 / src/prism.cu:9-192):
-// compress, decompress and progressive-decompress flows with file I/O and the
-// --report time,cr printouts.  Returns a process exit status.
+// Entry point of the PRISM flows (include/prism.hpp:5 of the reference):
+// initialize runs what the prism_context asks for -- compress, decompress,
+// or progressive decompress with its list of target errors -- reading and
+// writing the files it names and printing the --report lines.
 #pragma once
 #include "parameters.hpp"
 
-int initialize(prism_context* config);
+// Failures print the reason and end the process, as in the reference.
+void initialize(prism_context* config);
+// The same, returning 0 on success and nonzero after printing the reason.
+int prism_initialize(prism_context* config);

@@ -1,10 +1,11 @@
-// prism command-line tool (the reference's examples/prism.cpp).
+// prism command-line tool: the flow of the reference's examples/prism.cpp
+// (parse the flags, run the configured flows) with an exit status.
 #include "parameters.hpp"
 #include "prism.hpp"
 
 int main(int argc, char* argv[]) {
   prism_context config;
-  if (parse_argv(&config, argc, argv)) return 1;
+  if (prism_parse_argv(&config, argc, argv)) return 1;
   if (!config.isComp && !config.isDecomp) return 0;
-  return initialize(&config);
+  return prism_initialize(&config);
 }
