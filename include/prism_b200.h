@@ -123,6 +123,13 @@ int prism_progressive_step(prism_prog* p, double target_error, void* d_values, v
  * to the host while the next step runs. */
 int prism_progressive_step_into(prism_prog* p, double target_error, const void* d_prev, void* d_out,
                                 void* stream);
+/* Start an object from a state whose planes [0, end[l]) of every level are
+ * already reconstructed (values the caller holds, e.g. a cached earlier
+ * retrieval of the same container): the next step refines them, as the
+ * reference's later steps refine output_old into output_new
+ * (src/prism.cu:126-138, compressor.cu:166-190).  Only before the first step;
+ * the next step needs d_prev (prism_progressive_step_into). */
+int prism_progressive_resume(prism_prog* p, const int end[4], void* stream);
 /* begin/end/maxlevel after the last step; loaded = payload bytes of the
  * planes selected so far (calculate_accumulate_size, analyze.hpp:118-159). */
 int prism_progressive_state(const prism_prog* p, int begin[4], int end[4], int* maxlevel,
@@ -298,9 +305,16 @@ void prism_batch_destroy(prism_batch* b);
  * -prog containers and reconstructions resident on the current device and
  * answers "field f at error bound t" requests from `slots` worker threads
  * (one stream and workspace each) under an HBM budget.  A request's values are
- * those of a one-step progressive retrieval of f to t (prism_progressive_open
- * + one prism_progressive_step), whatever else is in flight; reconstructions
- * are cached per selected plane set and reused bit for bit. */
+ * the progressive retrieval of f to the planes that t selects: either one step
+ * from no planes (prism_progressive_open + one prism_progressive_step) or,
+ * when a reconstruction of f with a subset of those planes is resident, the
+ * reference's refinement step from it (prism_progressive_resume +
+ * prism_progressive_step_into; src/prism.cu:126-138).  The two carry the same
+ * planes and differ only by floating-point rounding of the refinement sum: at
+ * most 64 units in the last place of the field's largest magnitude
+ * (prism_server_set_refine(s, 0) makes every result the one-step retrieval,
+ * bit for bit).
+ * Reconstructions are cached per selected plane set and reused as they are. */
 typedef struct prism_server prism_server;
 typedef struct prism_server_stats {
   uint64_t completed, cache_hits, shared, evictions, failed;
@@ -308,6 +322,7 @@ typedef struct prism_server_stats {
   double p50_ms, p99_ms, mean_ms, max_ms, elapsed_s;  /* submit -> completion */
   double queue_p50_ms, queue_p99_ms;                  /* submit -> a slot takes it */
   double service_p50_ms, service_p99_ms;              /* slot start -> completion */
+  uint64_t refined;                                   /* misses refined from a coarser entry */
 } prism_server_stats;
 
 /* hbm_budget: bytes of device memory the server may hold (containers,
@@ -323,12 +338,16 @@ int prism_server_add_field(prism_server* s, const void* container, uint64_t size
 int prism_server_submit(prism_server* s, int field_id, double target_error, void* out, int out_on_device,
                         uint64_t* request_id);
 /* Wait for a request; latency = submit to completion.  end/maxlevel receive
- * the plane selection, from_cache whether a resident reconstruction served it.
- * Returns the request's status. */
+ * the plane selection; from_cache = 1 when a resident reconstruction served
+ * it, 2 when it was refined from a resident coarser one, 0 when computed from
+ * no planes.  Returns the request's status. */
 int prism_server_wait(prism_server* s, uint64_t request_id, double* latency_ms, int end[4], int* maxlevel,
                       int* from_cache);
 /* Non-blocking: *done = 1 once the request has completed (then wait). */
 int prism_server_poll(prism_server* s, uint64_t request_id, int* done);
+/* Refinement of misses from coarser resident entries: on (default) or off
+ * (every miss from no planes). */
+int prism_server_set_refine(prism_server* s, int enable);
 /* Latency percentiles and counters of the completed requests. */
 int prism_server_stats_get(prism_server* s, prism_server_stats* out, int reset);
 void prism_server_destroy(prism_server* s);

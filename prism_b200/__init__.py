@@ -77,6 +77,8 @@ def lib():
         l.prism_lossless_encode_static.argtypes = [vp, u32, u32, u32, vp, u64, C.POINTER(u64), vp, vp]
         l.prism_lossless_wait_selftest.argtypes = [vp, vp, u32, u32, u32, vp, u64, C.c_longlong, vp]
         l.prism_extrema_minmax.argtypes = [vp, vp, i32, u64, vp, vp]
+        l.prism_progressive_resume.argtypes = [vp, vp, vp]
+        l.prism_server_set_refine.argtypes = [vp, i32]
         l.prism_lost_codes.argtypes = [u32, u32, u32]
         l.prism_lost_codes.restype = u64
         l.prism_batch_create.argtypes = [vp, i32, i32, C.POINTER(vp)]
@@ -120,7 +122,7 @@ EXPORTED = [
     "prism_server_wait", "prism_server_stats_get", "prism_server_destroy", "prism_statistics", "prism_server_poll",
     "prism_file_save", "prism_file_open", "prism_file_step", "prism_file_info", "prism_file_close",
     "prism_progressive_step_into", "prism_profile_stages", "prism_lossless_wait_selftest", "prism_lost_codes",
-    "prism_extrema_minmax",
+    "prism_extrema_minmax", "prism_progressive_resume", "prism_server_set_refine",
 ]
 
 
@@ -298,6 +300,13 @@ class Progressive:
         self.comp.h.check(rc, "prism_progressive_step_into")
         return out
 
+    def resume(self, end):
+        """Start from values that hold planes [0, end[l]) of every level (before
+        the first step); the next step_into refines them."""
+        torch = _torch()
+        e = (C.c_int * 4)(*end)
+        self.comp.h.check(lib().prism_progressive_resume(self.ptr, e, _stream(torch)), "prism_progressive_resume")
+
     def state(self):
         """Plane state after the last step (waits for it; raises on a corrupt chunk)."""
         b = (C.c_int * 4)()
@@ -431,7 +440,8 @@ class ServerStats(C.Structure):
     _fields_ = [(k, C.c_uint64) for k in ("completed", "cache_hits", "shared", "evictions", "failed", "bytes_out",
                                           "bytes_resident", "bytes_reserved", "bytes_peak")] + \
                [(k, C.c_double) for k in ("p50_ms", "p99_ms", "mean_ms", "max_ms", "elapsed_s", "queue_p50_ms",
-                                          "queue_p99_ms", "service_p50_ms", "service_p99_ms")]
+                                          "queue_p99_ms", "service_p50_ms", "service_p99_ms")] + \
+               [("refined", C.c_uint64)]
 
 
 class Server:
@@ -459,6 +469,12 @@ class Server:
         self.fields.append(ctx)
         return fid.value
 
+    def refine(self, enable=True):
+        """Refine misses from resident coarser reconstructions (default on)."""
+        rc = lib().prism_server_set_refine(self.ptr, int(enable))
+        if rc:
+            raise PrismError(f"prism_server_set_refine: {_STATUS.get(rc, rc)}")
+
     def submit(self, field_id, target, out):
         """out: CUDA tensor (or numpy array) of the field's shape and dtype."""
         rid = C.c_uint64()
@@ -478,7 +494,8 @@ class Server:
         rc = lib().prism_server_wait(self.ptr, C.c_uint64(request_id), C.byref(lat), end, C.byref(ml), C.byref(hit))
         if rc:
             raise PrismError(f"prism_server_wait: {_STATUS.get(rc, rc)}")
-        return {"latency_ms": lat.value, "end": list(end), "maxlevel": ml.value, "from_cache": bool(hit.value)}
+        return {"latency_ms": lat.value, "end": list(end), "maxlevel": ml.value, "from_cache": hit.value == 1,
+                "refined": hit.value == 2}
 
     def done(self, request_id):
         d = C.c_int()

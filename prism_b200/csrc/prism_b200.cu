@@ -862,6 +862,15 @@ __global__ void prog_init_kernel(StrategyState* st, int* err) {
   if (threadIdx.x == 0) { st->maxlevel = 4; *err = 0; }
 }
 
+// the state of an object whose planes [0, end) are already reconstructed
+__global__ void prog_resume_kernel(StrategyState* st, int* err, int e0, int e1, int e2, int e3) {
+  if (threadIdx.x != 0) return;
+  const int e[4] = {e0, e1, e2, e3};
+  for (int i = 0; i < 4; ++i) { st->begin[i] = e[i]; st->end[i] = e[i]; }
+  st->maxlevel = 4;
+  *err = 0;
+}
+
 // The state after a step, for the host: plane ranges, error flag and the
 // payload bytes of every plane loaded so far.  Steps load [previous end,
 // end), so the total is planes [0, end) of each level, a difference of the
@@ -982,6 +991,22 @@ int prism_progressive_step_into(prism_prog* p, double target_error, const void* 
   cudaStream_t st = (cudaStream_t)stream;
   if (p->tsize == 4) return progressive_step_t<float>(p, target_error, (const float*)d_prev, (float*)d_out, st);
   return progressive_step_t<double>(p, target_error, (const double*)d_prev, (double*)d_out, st);
+}
+
+int prism_progressive_resume(prism_prog* p, const int end[4], void* stream) {
+  if (!p || !end) return PRISM_ERR_ARG;
+  if (p->steps != 0) return fail(p->h, PRISM_ERR_ARG, "resume applies to an object before its first step");
+  for (int i = 0; i < 4; ++i)
+    if (end[i] < 0 || end[i] > 32) return fail(p->h, PRISM_ERR_ARG, "plane ranges are 0..32");
+  cudaStream_t st = (cudaStream_t)stream;
+  prism_handle* h = p->h;
+  prog_resume_kernel<<<1, 32, 0, st>>>(p->d_state, p->d_err, end[0], end[1], end[2], end[3]);
+  h->launches += 1;
+  CK(cudaGetLastError());
+  for (int i = 0; i < 4; ++i) p->state.begin[i] = p->state.end[i] = end[i];
+  p->state.maxlevel = 4;
+  p->steps = 1;  // the next step adds to previous values, from zero anchors
+  return PRISM_OK;
 }
 
 int prism_progressive_state(const prism_prog* cp, int begin[4], int end[4], int* maxlevel, uint64_t* loaded) {

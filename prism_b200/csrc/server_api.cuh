@@ -3,12 +3,16 @@
 //
 // The server keeps compressed fields and their partial reconstructions
 // resident on the device and serves requests "field f at error bound t".
-// Each request is answered by the one-step progressive retrieval of f to t
-// (strategy from no planes to t, decode of the selected planes, inverse
-// shuffle, reconstruction), so its values depend only on (f, t) -- never on
-// the other requests in flight.  Reconstructions are cached per (field,
-// selected planes, max level): a request whose selection is cached or being
-// computed is served from that entry (bit-identical by construction).
+// A request's result is the reference's progressive retrieval of f to the
+// plane selection that t calls for (the strategy from no planes): either in
+// one step from no planes (strategy, decode of the selected planes, inverse
+// shuffle, reconstruction), or -- when a reconstruction of f with a coarser
+// selection is resident -- as the reference's refinement step from that
+// entry (src/prism.cu:126-138: output_old -> output_new, only the planes the
+// entry lacks are decoded and their delta added).  Both carry the same
+// planes; they differ only by the floating-point rounding of the refinement
+// sum.  Reconstructions are cached per (field, selected planes): a request
+// whose selection is cached or being computed is served from that entry.
 //
 // Continuous batching: `slots` worker threads, each with its own stream and
 // workspace, pull requests from one queue; a request is admitted when a slot
@@ -62,6 +66,7 @@ struct SrvRequest {
   int status = 0;
   bool done = false;
   bool hit = false;
+  bool refined = false;
   SrvClock::time_point t_submit, t_start, t_done;
   int end[4] = {0, 0, 0, 0};
   int maxlevel = 0;
@@ -94,10 +99,11 @@ struct prism_server {
   std::vector<std::unique_ptr<std::mutex>> slot_mu;  // held while a slot's handle is in use
   bool stop = false;
   bool warmed = false;
+  bool refine = true;  // misses refine the finest resident coarser entry of the field
   int device = 0;
   // statistics
   std::vector<double> lat_ms, queue_ms, service_ms;
-  uint64_t completed = 0, hits = 0, shared = 0, evictions = 0, failed = 0, bytes_out = 0;
+  uint64_t completed = 0, hits = 0, shared = 0, evictions = 0, failed = 0, bytes_out = 0, refined = 0;
   SrvClock::time_point t0;
   std::string err;
 };
@@ -147,8 +153,7 @@ void srv_worker(prism_server* s, int slot) {
     SrvEntry* e = nullptr;
     if (!rc) {
       for (auto& c : s->cache)
-        if (c.field == r->field && c.maxlevel == maxlevel && !c.failed &&
-            std::equal(c.end, c.end + 4, end)) {
+        if (c.field == r->field && !c.failed && std::equal(c.end, c.end + 4, end)) {
           e = &c;
           break;
         }
@@ -176,6 +181,29 @@ void srv_worker(prism_server* s, int slot) {
         if (!got) {
           rc = PRISM_ERR_NOMEM;
         } else {
+          // refinement base: the finest resident entry of the field whose
+          // planes are a subset of this selection (pinned while in use)
+          SrvEntry* base = nullptr;
+          int best = -1;
+          if (s->refine)
+            for (auto& c : s->cache) {
+              if (c.field != r->field || !c.ready || c.failed || std::equal(c.end, c.end + 4, end)) continue;
+              bool sub = true;
+              int sum = 0;
+              for (int l = 0; l < 4; ++l) {
+                sub &= c.end[l] <= end[l];
+                sum += c.end[l];
+              }
+              if (sub && sum > best) {
+                best = sum;
+                base = &c;
+              }
+            }
+          if (base) {
+            ++base->pins;
+            ++s->refined;
+            r->refined = true;
+          }
           s->cache.emplace_back();
           e = &s->cache.back();
           e->field = r->field;
@@ -183,15 +211,21 @@ void srv_worker(prism_server* s, int slot) {
           e->maxlevel = maxlevel;
           e->bytes = f.value_bytes;
           e->pins = 1;
+          const void* base_values = base ? base->d_values : nullptr;
+          int base_end[4] = {0, 0, 0, 0};
+          if (base) std::copy(base->end, base->end + 4, base_end);
           lk.unlock();
           void* p = nullptr;
           rc = cudaMallocAsync(&p, f.value_bytes, st) == cudaSuccess ? PRISM_OK : PRISM_ERR_NOMEM;
           prism_prog* pg = nullptr;
           if (!rc) rc = prism_progressive_open(h, f.d_cont, f.size, f.tsize, f.nx, f.ny, f.nz, f.mode, f.bound, &pg);
-          if (!rc) rc = prism_progressive_step(pg, r->target, p, st);
+          if (!rc && base) rc = prism_progressive_resume(pg, base_end, st);
+          if (!rc) rc = base ? prism_progressive_step_into(pg, r->target, base_values, p, st)
+                             : prism_progressive_step(pg, r->target, p, st);
           if (!rc) rc = prism_progressive_state(pg, nullptr, nullptr, nullptr, nullptr);  // waits, reports errors
           if (pg) prism_progressive_close(pg);
           lk.lock();
+          if (base) --base->pins;
           e->d_values = p;
           e->ready = true;
           e->failed = rc != 0;
@@ -383,7 +417,7 @@ int prism_server_wait(prism_server* s, uint64_t request_id, double* latency_ms, 
   if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
   if (end) std::copy(r->end, r->end + 4, end);
   if (maxlevel) *maxlevel = r->maxlevel;
-  if (from_cache) *from_cache = r->hit;
+  if (from_cache) *from_cache = r->hit ? 1 : (r->refined ? 2 : 0);
   int rc = r->status;
   s->reqs.erase(it);
   delete r;
@@ -413,6 +447,7 @@ int prism_server_stats_get(prism_server* s, prism_server_stats* out, int reset) 
   out->bytes_reserved = s->reserved;
   out->bytes_peak = s->peak;
   out->elapsed_s = std::chrono::duration<double>(SrvClock::now() - s->t0).count();
+  out->refined = s->refined;
   auto pct = [](std::vector<double> v, double p) {
     if (v.empty()) return 0.0;
     std::sort(v.begin(), v.end());
@@ -434,9 +469,16 @@ int prism_server_stats_get(prism_server* s, prism_server_stats* out, int reset) 
     s->lat_ms.clear();
     s->queue_ms.clear();
     s->service_ms.clear();
-    s->completed = s->hits = s->shared = s->evictions = s->failed = s->bytes_out = 0;
+    s->completed = s->hits = s->shared = s->evictions = s->failed = s->bytes_out = s->refined = 0;
     s->t0 = SrvClock::now();
   }
+  return PRISM_OK;
+}
+
+int prism_server_set_refine(prism_server* s, int enable) {
+  if (!s) return PRISM_ERR_ARG;
+  std::lock_guard<std::mutex> lk(s->m);
+  s->refine = enable != 0;
   return PRISM_OK;
 }
 
