@@ -538,6 +538,23 @@ def run_batched(torch, P, args):
     cbytes = sum(int(c.numel()) for c in conts)
     sch = b.schedule()
     b.close()
+    # every field decompressed: max error against its bound (REL 1e-3 of the
+    # field's range); fields whose shape makes the reference's last shuffle
+    # block drop code bits (prism_lost_codes > 0) are counted apart
+    worst, within, lost_fields, over_unflagged = 0.0, 0, 0, 0
+    for (ctx, d), c, comp in zip(items, ref, comps):  # ref: the per-field containers, equal to the batch's
+        rec = comp.decompress_pipeline(c)
+        st = h.statistics(d, rec)
+        eb = 1e-3 * (st["max"] - st["min"])
+        ratio = st["max_err"] / eb if eb > 0 else 0.0
+        lost = P.lost_codes(ctx.nx, ctx.ny, ctx.nz)
+        lost_fields += lost > 0
+        ok = bool(st["max_err"] <= eb * (1 + 1e-6) + 4 * float(np.finfo(np.float32).eps) *
+                  max(abs(st["min"]), abs(st["max"])))
+        within += ok
+        over_unflagged += (not ok) and lost == 0
+        worst = max(worst, float(ratio) if lost == 0 else 0.0)
+        del rec
     del items, outs, conts, ref
     return {"workload": "64 uneven float32 fields (1-D/2-D/3-D, extents log-uniform 32..2048, 3-D capped at "
                         "512^3 values, sinusoid sums and k^-5/3 fields alternating), REL 1e-3, compress",
@@ -545,6 +562,9 @@ def run_batched(torch, P, args):
             "batched_GBps": total / batch_ms / 1e6, "per_field_GBps": total / plain_ms / 1e6,
             "batched_ms": batch_ms, "per_field_ms": plain_ms, "speedup": plain_ms / batch_ms,
             "identical_containers": identical, "runs": reps, "plan_s": plan_s, "schedule": sch,
+            "fields_within_bound": within, "fields_with_lost_codes": lost_fields,
+            "fields_over_bound_without_lost_codes": over_unflagged,
+            "max_err_over_bound_unflagged": worst,
             "data": "synthetic, generated on the device"}
 
 

@@ -5,6 +5,8 @@ sign-magnitude/negabinary fields of uneven shapes."""
 import numpy as np
 import pytest
 
+import oracle as O
+
 pytestmark = pytest.mark.gpu
 
 # (kind, (nx, ny, nz), dtype, mode, bound, progressive)
@@ -28,7 +30,7 @@ def env():
     if not torch.cuda.is_available():
         pytest.skip("needs a CUDA device")
     from prism_b200 import fields
-    items, refs = [], []
+    items, refs, datas = [], [], []
     h = P.Handle()
     for i, (kind, (nx, ny, nz), dt, mode, bound, prog) in enumerate(MIX):
         data = fields.make(kind, (nz, ny, nx), dt, 10 + i)
@@ -38,13 +40,14 @@ def env():
         cont = comp.compress_pipeline(d_in).cpu().numpy().copy()
         items.append((ctx, d_in))
         refs.append((cont, comp.flags))
+        datas.append(data)
     torch.cuda.synchronize()
-    return torch, P, items, refs
+    return torch, P, items, refs, datas
 
 
 @pytest.mark.parametrize("use_graph", [True, False])
 def test_batch_matches_per_field_containers(env, use_graph):
-    torch, P, items, refs = env
+    torch, P, items, refs, _ = env
     b = P.Batch(items, use_graph=use_graph)
     for rep in range(2):
         conts, flags = b.compress()
@@ -64,7 +67,7 @@ def test_batch_matches_per_field_containers(env, use_graph):
 def test_batch_recompresses_new_contents(env):
     """The graph is bound to the buffers: new data in the same input buffers
     gives the per-field containers of the new data."""
-    torch, P, items, refs = env
+    torch, P, items, refs, _ = env
     b = P.Batch(items[:3], use_graph=True)
     b.compress()
     from prism_b200 import fields
@@ -82,3 +85,17 @@ def test_batch_recompresses_new_contents(env):
     for i, (ctx, d_in) in enumerate(items[:3]):
         kind, dims, dt = MIX[i][0], MIX[i][1], MIX[i][2]
         d_in.copy_(torch.from_numpy(fields.make(kind, (dims[2], dims[1], dims[0]), dt, 10 + i)))
+
+
+def test_batch_containers_match_oracle(env):
+    """Every batched container equals the oracle's container of that field
+    (with the batch's auto-tune decisions forced on the oracle), byte for
+    byte: the batched path against the reference's arithmetic directly."""
+    torch, P, items, refs, datas = env
+    b = P.Batch(items, use_graph=True)
+    conts, flags = b.compress()
+    for i, (kind, dims, dt, mode, bound, prog) in enumerate(MIX):
+        md, rv = flags[i]
+        ocont, _, _ = O.compress(datas[i], mode, bound, 0 if prog else 1, force=O.intp(md, rv))
+        assert conts[i].cpu().numpy().tobytes() == ocont, (i, MIX[i])
+    b.close()

@@ -4,6 +4,8 @@ container at every step and reads only the chunks of the planes it adds."""
 import numpy as np
 import pytest
 
+import oracle as O
+
 pytestmark = pytest.mark.gpu
 
 
@@ -32,11 +34,16 @@ def test_file_progressive_equals_memory(env, tmp_path, dt, mode, bound):
     fil = P.FileProgressive(P.Compressor(ctx), path)
     scale = 1.0 if mode == 1 else 1e-1
     reads = []
+    ost = O.ProgressiveState()
+    host = cont.cpu().numpy().tobytes()
     for t in [1e-1, 1e-3, 1e-5, 1e-6]:
         t = max(t * scale, bound)
         a = mem.step(t).clone()
         b = fil.step(t)
         assert torch.equal(a, b), t
+        # and the oracle's progressive chain, bit for bit
+        o, _ = O.progressive_step(host, (nz, ny, nx), dt, mode, bound, t, ost)
+        assert np.array_equal(b.cpu().numpy().view(np.uint8), o.view(np.uint8)), t
         reads.append(fil.info()["bytes_read"])
         assert fil.info()["end"] == mem.state()[1]
     info = fil.info()
