@@ -1178,7 +1178,7 @@ __device__ __forceinline__ void compress_tile(CompressSmem<T>& sm, const T* __re
 // do; double tiles (55 KB) and edge tiles are held to fewer by shared memory
 // and their runtime limits.
 template <class T, int PART>
-constexpr int predict_min_ctas() { return sizeof(T) == 4 && PART == 0 ? 6 : 3; }
+constexpr int predict_min_ctas() { return sizeof(T) == 4 && PART == 0 ? 6 : 4; }
 
 template <class T, int PART>
 __global__ void __launch_bounds__(kPredThreads, predict_min_ctas<T, PART>())
@@ -1198,7 +1198,7 @@ predict_compress_kernel(const T* __restrict__ data, Geometry g, const PredParams
 // a float interior tile's 23 KB of shared memory leaves room for seven
 // CTAs on an SM when its registers do; a double one (43 KB) for five
 template <class T, int PART>
-constexpr int reconstruct_min_ctas() { return PART == 0 ? (sizeof(T) == 4 ? 7 : 5) : 3; }
+constexpr int reconstruct_min_ctas() { return PART == 0 ? (sizeof(T) == 4 ? 7 : 5) : 4; }
 
 template <class T, bool PROG, int PART>
 __global__ void __launch_bounds__(kPredThreads, reconstruct_min_ctas<T, PART>())
