@@ -130,6 +130,24 @@ int prism_progressive_step_into(prism_prog* p, double target_error, const void* 
  * (src/prism.cu:126-138, compressor.cu:166-190).  Only before the first step;
  * the next step needs d_prev (prism_progressive_step_into). */
 int prism_progressive_resume(prism_prog* p, const int end[4], void* stream);
+/* Exact refinement (no counterpart in the reference; off by default, which is
+ * the reference's behaviour).  The container's chunks are cut at the host
+ * plane stride, which can exceed the device stride the planes are laid out
+ * with (by 8 bytes per plane when a plane's size is a multiple of 8 bytes,
+ * plus 256 bytes per earlier level), so the first bytes of device plane b can
+ * lie in the chunks of plane b - 1.  A reference step that loads planes
+ * [b, e) decodes the chunks of planes b..e-1 only, and the step that loaded
+ * plane b - 1 masked plane b out: a chained retrieval never sees those bytes,
+ * its values differ from the one-step retrieval to the same planes and can
+ * miss the requested bound (on a 64x48x40 double field the chain 1e-2 ->
+ * 1e-4 ends 0.45% of the range away from the data).  With
+ * exact mode on, a step also decodes the chunks of plane b - 1 of every level
+ * that gains planes and keeps planes [b, e) of them, so after every step the
+ * values hold complete device planes [0, e) and equal the one-step retrieval
+ * up to the rounding of the sum (when the object starts from values that
+ * hold complete planes: a first step, an exact step, or a resume from
+ * either).  Set before the step it should apply to. */
+int prism_progressive_exact(prism_prog* p, int enable);
 /* begin/end/maxlevel after the last step; loaded = payload bytes of the
  * planes selected so far (calculate_accumulate_size, analyze.hpp:118-159). */
 int prism_progressive_state(const prism_prog* p, int begin[4], int end[4], int* maxlevel,
@@ -307,11 +325,12 @@ void prism_batch_destroy(prism_batch* b);
  * (one stream and workspace each) under an HBM budget.  A request's values are
  * the progressive retrieval of f to the planes that t selects: either one step
  * from no planes (prism_progressive_open + one prism_progressive_step) or,
- * when a reconstruction of f with a subset of those planes is resident, the
- * reference's refinement step from it (prism_progressive_resume +
- * prism_progressive_step_into; src/prism.cu:126-138).  The two carry the same
- * planes and differ only by floating-point rounding of the refinement sum: at
- * most 64 units in the last place of the field's largest magnitude
+ * when a reconstruction of f with a subset of those planes is resident, a
+ * refinement step from it (prism_progressive_resume +
+ * prism_progressive_step_into, src/prism.cu:126-138, in exact mode:
+ * prism_progressive_exact).  The two carry the same planes and differ only by
+ * floating-point rounding of the refinement sum: at most 64 units in the last
+ * place of the field's largest magnitude
  * (prism_server_set_refine(s, 0) makes every result the one-step retrieval,
  * bit for bit).
  * Reconstructions are cached per selected plane set and reused as they are. */

@@ -148,12 +148,14 @@ class ProgressiveState:
         self.prev = None
 
 
-def progressive_step(cont, shape, dtype, mode, bound, target, state):
+def progressive_step(cont, shape, dtype, mode, bound, target, state, exact=False):
+    """One step of the reference's progressive retrieval; exact=True is this
+    library's exact refinement (or_progressive_step_exact)."""
     nz, ny, nx = shape
     buf = np.frombuffer(cont, dtype=np.uint8).copy()
     out = np.zeros(shape, dtype=dtype)
     old = state.prev if state.prev is not None else np.zeros(shape, dtype=dtype)
-    rc = getattr(lib(), "or_progressive_step_" + _suffix(dtype))(
+    rc = getattr(lib(), ("or_progressive_step_exact_" if exact else "or_progressive_step_") + _suffix(dtype))(
         _p(buf), C.c_uint64(len(cont)), C.c_uint32(nx), C.c_uint32(ny), C.c_uint32(nz),
         C.c_int(mode), C.c_double(bound), C.c_double(target), C.c_double(state.last),
         state.begin, state.end, C.byref(state.maxlevel), _p(old), _p(out))

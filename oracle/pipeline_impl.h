@@ -97,9 +97,10 @@ int FN(or_decompress)(const uint8_t* cont, uint64_t size, uint32_t nx, uint32_t 
   return 0;
 }
 
-int FN(or_progressive_step)(const uint8_t* cont, uint64_t size, uint32_t nx, uint32_t ny,
-                            uint32_t nz, int mode, double bound, double target, double last,
-                            int begin[4], int end[4], int* maxlevel, const T* old, T* out) {
+static int FN(progressive_step_impl)(const uint8_t* cont, uint64_t size, uint32_t nx, uint32_t ny,
+                                     uint32_t nz, int mode, double bound, double target, double last,
+                                     int begin[4], int end[4], int* maxlevel, const T* old, T* out,
+                                     int exact) {
   or_geom g;
   or_geometry(nx, ny, nz, (int)sizeof(T), &g);
   or_intp p; double range; uint64_t csbp[128]; const uint8_t* ap;
@@ -112,7 +113,9 @@ int FN(or_progressive_step)(const uint8_t* cont, uint64_t size, uint32_t nx, uin
   p.beta = 4.0;
   or_find_strategy(csbp, eb, target, begin, end, maxlevel);
   uint8_t* planes = FN(alloc_planes)(&g);
-  rc = or_zbpc_decode_progressive(cont, &g, begin, end, planes);
+  int dec_begin[4];
+  for (int i = 0; i < 4; ++i) dec_begin[i] = exact && begin[i] > 0 && begin[i] < end[i] ? begin[i] - 1 : begin[i];
+  rc = or_zbpc_decode_progressive(cont, &g, dec_begin, end, planes);
   if (rc) { free(planes); return rc; }
   int32_t* qc = FN(alloc_qc)(&g);
   or_inverse_bitshuffle_progressive(planes, &g, begin, end, qc);
@@ -121,4 +124,18 @@ int FN(or_progressive_step)(const uint8_t* cont, uint64_t size, uint32_t nx, uin
   FN(or_reconstruct)(qc, anchors, &g, eb, &p, *maxlevel, first ? NULL : old, out);
   free(anchors); free(qc); free(planes);
   return 0;
+}
+
+int FN(or_progressive_step)(const uint8_t* cont, uint64_t size, uint32_t nx, uint32_t ny,
+                            uint32_t nz, int mode, double bound, double target, double last,
+                            int begin[4], int end[4], int* maxlevel, const T* old, T* out) {
+  return FN(progressive_step_impl)(cont, size, nx, ny, nz, mode, bound, target, last, begin, end, maxlevel, old,
+                                   out, 0);
+}
+
+int FN(or_progressive_step_exact)(const uint8_t* cont, uint64_t size, uint32_t nx, uint32_t ny,
+                                  uint32_t nz, int mode, double bound, double target, double last,
+                                  int begin[4], int end[4], int* maxlevel, const T* old, T* out) {
+  return FN(progressive_step_impl)(cont, size, nx, ny, nz, mode, bound, target, last, begin, end, maxlevel, old,
+                                   out, 1);
 }

@@ -165,6 +165,16 @@ int or_progressive_step_f32(const uint8_t* cont, uint64_t size, uint32_t nx, uin
 int or_progressive_step_f64(const uint8_t* cont, uint64_t size, uint32_t nx, uint32_t ny,
                             uint32_t nz, int mode, double bound, double target, double last,
                             int begin[4], int end[4], int* maxlevel, const double* old, double* out);
+/* The same step in this library's exact refinement (prism_progressive_exact;
+ * not a reference behaviour): a later step also decodes the chunks of plane
+ * begin - 1 of every level that gains planes, and the inverse shuffle keeps
+ * planes [begin, end) of what was decoded. */
+int or_progressive_step_exact_f32(const uint8_t* cont, uint64_t size, uint32_t nx, uint32_t ny,
+                                  uint32_t nz, int mode, double bound, double target, double last,
+                                  int begin[4], int end[4], int* maxlevel, const float* old, float* out);
+int or_progressive_step_exact_f64(const uint8_t* cont, uint64_t size, uint32_t nx, uint32_t ny,
+                                  uint32_t nz, int mode, double bound, double target, double last,
+                                  int begin[4], int end[4], int* maxlevel, const double* old, double* out);
 
 #ifdef __cplusplus
 }

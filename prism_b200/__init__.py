@@ -78,6 +78,7 @@ def lib():
         l.prism_lossless_wait_selftest.argtypes = [vp, vp, u32, u32, u32, vp, u64, C.c_longlong, vp]
         l.prism_extrema_minmax.argtypes = [vp, vp, i32, u64, vp, vp]
         l.prism_progressive_resume.argtypes = [vp, vp, vp]
+        l.prism_progressive_exact.argtypes = [vp, C.c_int]
         l.prism_server_set_refine.argtypes = [vp, i32]
         l.prism_lost_codes.argtypes = [u32, u32, u32]
         l.prism_lost_codes.restype = u64
@@ -122,7 +123,7 @@ EXPORTED = [
     "prism_server_wait", "prism_server_stats_get", "prism_server_destroy", "prism_statistics", "prism_server_poll",
     "prism_file_save", "prism_file_open", "prism_file_step", "prism_file_info", "prism_file_close",
     "prism_progressive_step_into", "prism_profile_stages", "prism_lossless_wait_selftest", "prism_lost_codes",
-    "prism_extrema_minmax", "prism_progressive_resume", "prism_server_set_refine",
+    "prism_extrema_minmax", "prism_progressive_resume", "prism_progressive_exact", "prism_server_set_refine",
 ]
 
 
@@ -306,6 +307,12 @@ class Progressive:
         torch = _torch()
         e = (C.c_int * 4)(*end)
         self.comp.h.check(lib().prism_progressive_resume(self.ptr, e, _stream(torch)), "prism_progressive_resume")
+
+    def exact(self, enable=True):
+        """Exact refinement (prism_progressive_exact): later steps also decode
+        the chunks of the plane below their range, so every step's values
+        equal the one-step retrieval to its planes up to rounding."""
+        self.comp.h.check(lib().prism_progressive_exact(self.ptr, int(bool(enable))), "prism_progressive_exact")
 
     def state(self):
         """Plane state after the last step (waits for it; raises on a corrupt chunk)."""

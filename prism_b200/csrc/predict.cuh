@@ -87,6 +87,52 @@ struct Expr {
 constexpr int kWin = 17;
 constexpr int kWinVol = kWin * kWin * kWin;
 
+// Window layout of the tile kernels: the slot of window point (x, y, z) is
+//   x + 17 y + (y >> 1) + RZ z + SZ (z >> 1)
+// (double: RZ = 297, SZ = 0, 5049 slots; float: RZ = 299, SZ = 3, 5105).
+// Every stage of a sweep touches points of one parity class; in a plain
+// 17^3 layout their slots differ by even multiples of the pitches, so a warp
+// uses half of the shared-memory banks (double: 8 of the 16 bank pairs) and
+// each access costs at least twice its wavefronts.  The skews after every
+// second row and plane spread a class over all banks.  The constants minimise
+// the wavefronts of the level-0 stages' lane-by-lane accesses over this
+// family of layouts (with the stage-to-lane maps below), within the
+// shared-memory budget of four double compression tiles per SM.
+template <class T>
+struct Win {
+  static constexpr int RY = 17, SY = 1;
+  static constexpr int RZ = sizeof(T) == 8 ? 297 : 299, SZ = sizeof(T) == 8 ? 0 : 3;
+  // the part of a slot that coordinate c along axis d contributes
+  static __host__ __device__ constexpr int axis(int d, int c) {
+    return d == 0 ? c : (d == 1 ? RY * c + SY * (c >> 1) : RZ * c + SZ * (c >> 1));
+  }
+  static __host__ __device__ constexpr int at(int x, int y, int z) { return axis(0, x) + axis(1, y) + axis(2, z); }
+  static constexpr int kSize = at(16, 16, 16) + 1;
+  // slots between coordinates c and c + 2 along axis d (the same for every c)
+  static __host__ __device__ constexpr int step2(int d) { return d == 0 ? 2 : (d == 1 ? 2 * RY + SY : 2 * RZ + SZ); }
+  // slots between coordinates 2m and 2m + 1 along axis d
+  static __host__ __device__ constexpr int one(int d) { return d == 0 ? 1 : (d == 1 ? RY : RZ); }
+  static __host__ __device__ constexpr int skew(int d) { return d == 0 ? 0 : (d == 1 ? SY : SZ); }
+};
+
+// Slot offsets of the neighbours -3u, -u, +u, +3u of a point along one axis.
+// Around an odd coordinate (u = 1) the skew makes them uneven; around an even
+// coordinate with an even unit u they are multiples of step2.
+struct Nb {
+  int m3, m1, p1, p3;
+};
+template <class T>
+__device__ __forceinline__ Nb nb_odd(int d) {
+  using W = Win<T>;
+  const int r = W::one(d), k = W::skew(d);
+  return {-3 * r - k, -r, r + k, 3 * r + 2 * k};
+}
+template <class T>
+__device__ __forceinline__ Nb nb_even(int d, int u) {
+  const int s = (u >> 1) * Win<T>::step2(d);
+  return {-3 * s, -s, s, 3 * s};
+}
+
 // FAST marks an interior tile: its whole 17^3 window lies inside the field and
 // it is not the last tile along any axis, so every boundary test below folds
 // to a constant.  Both forms evaluate the same expressions on the same values.
@@ -306,22 +352,27 @@ __device__ __forceinline__ int order_of(const Limits<EDGE>& L, int c) {
   return b ? (f3 ? 4 : (f1 ? 3 : 0)) : (f3 ? 2 : (f1 ? 1 : 0));
 }
 
-constexpr int kStride[3] = {1, kWin, kWin * kWin};
+// window slots between coordinates c and c + U along axis D, U even
+template <class T, int U, int D>
+constexpr int unit_stride() {
+  static_assert(U % 2 == 0, "even units");
+  return (U / 2) * Win<T>::step2(D);
+}
 
 // 1-D prediction along window axis D at coordinate c (pred_line :1300-1326)
 template <class T, int U, int D, bool MD>
 __device__ __forceinline__ T line_at(const T* w, int o, bool nat) {
   using E = Expr<T>;
-  constexpr int S = kStride[D];
-  const T t1 = w[-U * S];
+  constexpr int S = unit_stride<T, U, D>();
+  const T t1 = w[-S];
   if (o == 0) return t1;
-  const T t2 = w[U * S];
+  const T t2 = w[S];
   if (o == 4) {
-    const T t0 = w[-3 * U * S], t3 = w[3 * U * S];
+    const T t0 = w[-3 * S], t3 = w[3 * S];
     return MD ? E::cubic_lambda(t0, t1, t2, t3, nat) : E::cubic_axis(t0, t1, t2, t3, nat);
   }
-  if (o == 3) return E::quad_l(w[-3 * U * S], t1, t2);
-  if (o == 2) return E::quad_r(t1, t2, w[3 * U * S]);
+  if (o == 3) return E::quad_l(w[-3 * S], t1, t2);
+  if (o == 2) return E::quad_r(t1, t2, w[3 * S]);
   return E::lin(t1, t2);
 }
 
@@ -341,8 +392,8 @@ __device__ __forceinline__ T face_at(const T* w, int o1, int o2, bool nat) {
     return E::half(F::add(line_at<T, U, D1, true>(w, o1, nat), line_at<T, U, D2, true>(w, o2, nat)));
   if (o1 >= 2 || (o1 == 1 && o2 == 0)) return line_at<T, U, D1, true>(w, o1, nat);
   if (o2 >= 1) return line_at<T, U, D2, true>(w, o2, nat);
-  constexpr int S1 = kStride[D1], S2 = kStride[D2];
-  return F::sub(F::add(w[-U * S1], w[-U * S2]), w[-U * S1 - U * S2]);
+  constexpr int S1 = unit_stride<T, U, D1>(), S2 = unit_stride<T, U, D2>();
+  return F::sub(F::add(w[-S1], w[-S2]), w[-S1 - S2]);
 }
 
 // CUBE (:1671-1723)
@@ -351,8 +402,8 @@ __device__ __forceinline__ T cube_at(const T* w, int ox, int oy, int oz, bool na
   using E = Expr<T>;
   using F = Fp<T>;
   auto cub = [&](auto D) {
-    constexpr int s = kStride[decltype(D)::value];
-    return E::cubic_lambda(w[-3 * U * s], w[-U * s], w[U * s], w[3 * U * s], nat);
+    constexpr int s = unit_stride<T, U, decltype(D)::value>();
+    return E::cubic_lambda(w[-3 * s], w[-s], w[s], w[3 * s], nat);
   };
   using DX = std::integral_constant<int, 0>;
   using DY = std::integral_constant<int, 1>;
@@ -364,10 +415,11 @@ __device__ __forceinline__ T cube_at(const T* w, int ox, int oy, int oz, bool na
   if (oz == 4) return cub(DZ());
   if (oy == 4) return cub(DY());
   if (ox == 4) return cub(DX());
-  if (ox == 3) return E::quad_l(w[-3 * U], w[-U], w[U]);
-  if (ox == 2) return E::quad_r_cube(w[-U], w[U], w[3 * U]);
-  if (ox == 1) return E::lin(w[-U], w[U]);
-  return w[-U];
+  constexpr int SX = unit_stride<T, U, 0>();
+  if (ox == 3) return E::quad_l(w[-3 * SX], w[-SX], w[SX]);
+  if (ox == 2) return E::quad_r_cube(w[-SX], w[SX], w[3 * SX]);
+  if (ox == 1) return E::lin(w[-SX], w[SX]);
+  return w[-SX];
 }
 
 // One level (unit U) of a tile sweep.
@@ -432,7 +484,7 @@ struct LevelSweep {
       c[A1] = U * (k1 * ST1 + OF1);
       c[A2] = U * (k2 * ST2 + OF2);
       if (!pred_ok(c, exclusive)) continue;
-      const int wi = (c[2] * kWin + c[1]) * kWin + c[0];
+      const int wi = Win<T>::at(c[0], c[1], c[2]);
       emit(wi, c, line_at<T, U, AX, MD>(win + wi, order_of<U, EDGE, AX>(L, c[AX]), nat));
     }
     if (SYNC) __syncthreads();
@@ -450,7 +502,7 @@ struct LevelSweep {
       c[P1] = 2 * U * k1 + U;
       c[P2] = 2 * U * k2 + U;
       if (!pred_ok(c, false)) continue;
-      const int wi = (c[2] * kWin + c[1]) * kWin + c[0];
+      const int wi = Win<T>::at(c[0], c[1], c[2]);
       emit(wi, c, face_at<T, U, P1, P2>(win + wi, order_of<U, EDGE, P1>(L, c[P1]), order_of<U, EDGE, P2>(L, c[P2]),
                                       nat));
     }
@@ -462,7 +514,7 @@ struct LevelSweep {
     for (int i = threadIdx.x; i < total; i += kPredThreads) {
       int c[3] = {2 * U * (i % N) + U, 2 * U * ((i / N) % N) + U, 2 * U * (i / (N * N)) + U};
       if (!pred_ok(c, exclusive)) continue;
-      const int wi = (c[2] * kWin + c[1]) * kWin + c[0];
+      const int wi = Win<T>::at(c[0], c[1], c[2]);
       emit(wi, c, cube_at<T, U>(win + wi, order_of<U, EDGE, 0>(L, c[0]), order_of<U, EDGE, 1>(L, c[1]),
                              order_of<U, EDGE, 2>(L, c[2]), nat));
     }
@@ -477,12 +529,16 @@ struct LevelSweep {
   // quadratic from the left, cubic in between.
   // order along an axis at odd coordinate c of an interior tile, level 0
   static __device__ __forceinline__ int order0(int c) { return c == 1 ? 2 : (c == 15 ? 3 : 4); }
-  // ---- md level 0 of an interior tile by jobs along one odd axis ----------
-  // A job walks the odd points 2j+1, j in [j0, j1), of a line with window
-  // stride S, holding the line's even values E[j-1..j+2] in a sliding window
-  // (compact code: one instance serves every axis).  cwi/cs locate the
-  // points' codes in the tile's 16^3 code block; `own` tells whether the
-  // line's fixed coordinates lie in the tile's own region.
+  // ---- level 0 of an interior tile by jobs along one odd axis ------------
+  // A job predicts the odd points 2j+1, j in [j0, j1), of a line with window
+  // stride S.  cw0/cs locate the points' codes in the tile's 16^3 code block;
+  // `own` tells whether the line's fixed coordinates lie in the tile's own
+  // region.  Points go in groups: a group first reads every value it needs
+  // (the line's even values E[g-1 .. g+G+1], its points' codes -- compression:
+  // their original values -- and, for faces, the neighbours on the second
+  // line), then predicts, then writes.  No point of a stage reads a point of
+  // the same stage, so the reads of a group are in flight together instead
+  // of each waiting behind the previous point's write.
   __device__ __forceinline__ void emit_at(int wi, int cwi, bool own, T pred) const {
     if (COMPRESS) {
       T rec;
@@ -493,112 +549,130 @@ struct LevelSweep {
       win[wi] = Fp<T>::fma(code_of(wi), ebx2, pred);
     }
   }
-  // line_at (MD) along a runtime stride with an interior order
-  __device__ __forceinline__ T line_md_rt(const T* w, int S, int o) const {
-    using E = Expr<T>;
-    const T t1 = w[-S], t2 = w[S];
-    if (o == 4) return E::cubic_lambda(w[-3 * S], t1, t2, w[3 * S], nat);
-    if (o == 3) return E::quad_l(w[-3 * S], t1, t2);
-    return E::quad_r(t1, t2, w[3 * S]);
+  // emit_at with the point's code (compression: its original value) read
+  // beforehand
+  __device__ __forceinline__ void emit_read(int wi, int cwi, bool own, T v, T pred) const {
+    if (COMPRESS) {
+      T rec;
+      const int32_t code = quantize(v, pred, ebr, ebx2, &rec);
+      if (own) cw[cwi] = code;
+      win[wi] = rec;
+    } else {
+      win[wi] = Fp<T>::fma(v, ebx2, pred);
+    }
   }
+  __device__ __forceinline__ T read_point(int wi) const { return COMPRESS ? win[wi] : code_of(wi); }
   // KIND 0: md line points (prediction along the job axis only);
   // KIND 2: per-axis points (the same with the per-axis cubic);
   // KIND 1: md faces, the job axis J and a second odd axis with stride SK
   // and order ok (face_at: both cubic -> the mean of the two lines, one cubic
   // -> that line, neither -> the mean; add() is commutative bit for bit).
-  // Point j of a job with its order OJ along the job axis (interior orders:
-  // j = 0 quadratic from the right, j = 7 from the left, cubic in between).
-  template <int KIND, int OJ>
-  __device__ __forceinline__ void md_point(int j, int w0, int S, int cw0, int cs, bool own, int SK, int ok, T p,
-                                           T a, T b, T c) const {
-    using E = Expr<T>;
-    using F = Fp<T>;
-    const int wi = w0 + (2 * j + 1) * S;
-    const T lj = OJ == 4 ? (KIND == 2 ? E::cubic_axis(p, a, b, c, nat) : E::cubic_lambda(p, a, b, c, nat))
-                         : (OJ == 2 ? E::quad_r(a, b, c) : E::quad_l(p, a, b));
-    T pred = lj;
-    if (KIND == 1 && !(OJ == 4 && ok != 4)) {
-      const T lk = line_md_rt(win + wi, SK, ok);
-      pred = (OJ != 4 && ok == 4) ? lk : E::half(F::add(lj, lk));
-    }
-    emit_at(wi, cw0 + (2 * j + 1) * cs, own, pred);
-  }
-  // The first and last points are peeled off the loop, so inside it the
-  // order is a constant and a point costs no order branches.
+  // Interior orders along the job axis: j = 0 quadratic from the right, j = 7
+  // from the left, cubic in between.  j0 and j1 are multiples of the group.
+  // w0: the slot of the line's point at coordinate 0 along the job axis J;
+  // K: the second odd axis of a face job.
   template <int KIND>
-  __device__ __forceinline__ void md_job(int w0, int S, int cw0, int cs, bool own, int j0, int j1, int SK,
+  __device__ __forceinline__ void md_job(int w0, int J, int cw0, int cs, bool own, int j0, int j1, int K,
                                          int ok) const {
-    T p = j0 > 0 ? win[w0 + 2 * (j0 - 1) * S] : T(0);
-    T a = win[w0 + 2 * j0 * S], b = win[w0 + 2 * (j0 + 1) * S];
-    T c = j0 + 2 <= 8 ? win[w0 + 2 * (j0 + 2) * S] : T(0);
-    int j = j0;
-    if (j == 0 && j < j1) {
-      md_point<KIND, 2>(0, w0, S, cw0, cs, own, SK, ok, p, a, b, c);
-      p = a;
-      a = b;
-      b = c;
-      c = win[w0 + 6 * S];
-      j = 1;
-    }
-    const int jm = j1 < 7 ? j1 : 7;
-#pragma unroll 1
-    for (; j < jm; ++j) {
-      md_point<KIND, 4>(j, w0, S, cw0, cs, own, SK, ok, p, a, b, c);
-      p = a;
-      a = b;
-      b = c;
-      if (j + 3 <= 8) c = win[w0 + 2 * (j + 3) * S];
-    }
-    if (j == 7 && j1 == 8) md_point<KIND, 3>(7, w0, S, cw0, cs, own, SK, ok, p, a, b, c);
-  }
-  // md cube points (x odd, cy, cz) along x, cube_at's cases for interior
-  // orders with its summation order for three cubics
-  __device__ __forceinline__ void md_cube_job(int cy, int cz, int j0, int j1) const {
     using E = Expr<T>;
     using F = Fp<T>;
-    constexpr int SY = kWin, SZ = kWin * kWin;
-    const int w0 = (cz * kWin + cy) * kWin, cw0 = (cz * 16 + cy) * 16;
+    constexpr int G = KIND == 1 ? 2 : 4;
+    const int E2 = Win<T>::step2(J), O1 = Win<T>::one(J);  // even point e at w0 + e E2, odd point j at + O1
+    const Nb nk = nb_odd<T>(K);
+#pragma unroll
+    for (int g = 0; g < 8; g += G) {
+      if (g < j0 || g >= j1) continue;
+      T ev[G + 3];  // E[g - 1 + k]
+#pragma unroll
+      for (int k = 0; k < G + 3; ++k) {
+        const int e = g - 1 + k;
+        ev[k] = e >= 0 && e <= 8 ? win[w0 + e * E2] : T(0);
+      }
+      T v[G], k0[G], k1[G], k2[G], k3[G];  // faces: the second line at -3, -1, +1, +3
+#pragma unroll
+      for (int i = 0; i < G; ++i) {
+        const int j = g + i;
+        const int wi = w0 + j * E2 + O1;
+        v[i] = read_point(wi);
+        // the second line is read where face_at uses it: unless the job
+        // axis alone is cubic
+        if (KIND == 1 && (ok == 4 || j == 0 || j == 7)) {
+          k1[i] = win[wi + nk.m1];
+          k2[i] = win[wi + nk.p1];
+          k0[i] = ok != 2 ? win[wi + nk.m3] : T(0);
+          k3[i] = ok != 3 ? win[wi + nk.p3] : T(0);
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < G; ++i) {
+        const int j = g + i;
+        const int oj = j == 0 ? 2 : (j == 7 ? 3 : 4);
+        const T lj = oj == 4 ? (KIND == 2 ? E::cubic_axis(ev[i], ev[i + 1], ev[i + 2], ev[i + 3], nat)
+                                          : E::cubic_lambda(ev[i], ev[i + 1], ev[i + 2], ev[i + 3], nat))
+                             : (oj == 2 ? E::quad_r(ev[i + 1], ev[i + 2], ev[i + 3]) : E::quad_l(ev[i], ev[i + 1], ev[i + 2]));
+        T pred = lj;
+        if (KIND == 1 && !(oj == 4 && ok != 4)) {
+          const T lk = ok == 4 ? E::cubic_lambda(k0[i], k1[i], k2[i], k3[i], nat)
+                               : (ok == 3 ? E::quad_l(k0[i], k1[i], k2[i]) : E::quad_r(k1[i], k2[i], k3[i]));
+          pred = (oj != 4 && ok == 4) ? lk : E::half(F::add(lj, lk));
+        }
+        emit_read(w0 + j * E2 + O1, cw0 + (2 * j + 1) * cs, own, v[i], pred);
+      }
+    }
+  }
+  // md cube points (x odd, cy, cz) along x, j in [j0, j0 + 2): cube_at's
+  // cases for interior orders with its summation order for three cubics.
+  // The reads of both points come first (the directions along y and z only
+  // where they are cubic).
+  __device__ __forceinline__ void md_cube_job(int cy, int cz, int j0) const {
+    using E = Expr<T>;
+    using F = Fp<T>;
+    const int w0 = Win<T>::at(0, cy, cz), cw0 = (cz * 16 + cy) * 16;
     const int oy = order0(cy), oz = order0(cz);
-    T p = j0 > 0 ? win[w0 + 2 * (j0 - 1)] : T(0);
-    T a = win[w0 + 2 * j0], b = win[w0 + 2 * (j0 + 1)];
-    T c = j0 + 2 <= 8 ? win[w0 + 2 * (j0 + 2)] : T(0);
-#pragma unroll 1
-    for (int j = j0; j < j1; ++j) {
-      const int wi = w0 + 2 * j + 1;
-      const T* w = win + wi;
+    const Nb ny = nb_odd<T>(1), nz = nb_odd<T>(2);
+    T ev[5];  // E[j0 - 1 + k] along x
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      const int e = j0 - 1 + k;
+      ev[k] = e >= 0 && e <= 8 ? win[w0 + 2 * e] : T(0);
+    }
+    T v[2], ya[2][4], za[2][4];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const int wi = w0 + 2 * (j0 + i) + 1;
+      v[i] = read_point(wi);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int dy = k == 0 ? ny.m3 : (k == 1 ? ny.m1 : (k == 2 ? ny.p1 : ny.p3));
+        const int dz = k == 0 ? nz.m3 : (k == 1 ? nz.m1 : (k == 2 ? nz.p1 : nz.p3));
+        ya[i][k] = oy == 4 ? win[wi + dy] : T(0);
+        za[i][k] = oz == 4 ? win[wi + dz] : T(0);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const int j = j0 + i;
       const int ox = j == 0 ? 2 : (j == 7 ? 3 : 4);
+      const T p = ev[i], a = ev[i + 1], b = ev[i + 2], c = ev[i + 3];
+      auto cyf = [&]() { return E::cubic_lambda(ya[i][0], ya[i][1], ya[i][2], ya[i][3], nat); };
+      auto czf = [&]() { return E::cubic_lambda(za[i][0], za[i][1], za[i][2], za[i][3], nat); };
       T pred;
       if (ox == 4) {
         const T cx = E::cubic_lambda(p, a, b, c, nat);
-        if (oz == 4 && oy == 4) {
-          const T cy_ = E::cubic_lambda(w[-3 * SY], w[-SY], w[SY], w[3 * SY], nat);
-          const T cz_ = E::cubic_lambda(w[-3 * SZ], w[-SZ], w[SZ], w[3 * SZ], nat);
-          pred = F::div(F::add(F::add(cx, cy_), cz_), T(3));
-        } else if (oz == 4) {
-          pred = E::half(F::add(E::cubic_lambda(w[-3 * SZ], w[-SZ], w[SZ], w[3 * SZ], nat), cx));
-        } else if (oy == 4) {
-          pred = E::half(F::add(E::cubic_lambda(w[-3 * SY], w[-SY], w[SY], w[3 * SY], nat), cx));
-        } else {
-          pred = cx;
-        }
+        if (oz == 4 && oy == 4) pred = F::div(F::add(F::add(cx, cyf()), czf()), T(3));
+        else if (oz == 4) pred = E::half(F::add(czf(), cx));
+        else if (oy == 4) pred = E::half(F::add(cyf(), cx));
+        else pred = cx;
       } else if (oz == 4 || oy == 4) {
-        if (oz == 4 && oy == 4)
-          pred = E::half(F::add(E::cubic_lambda(w[-3 * SZ], w[-SZ], w[SZ], w[3 * SZ], nat),
-                                E::cubic_lambda(w[-3 * SY], w[-SY], w[SY], w[3 * SY], nat)));
-        else if (oz == 4)
-          pred = E::cubic_lambda(w[-3 * SZ], w[-SZ], w[SZ], w[3 * SZ], nat);
-        else
-          pred = E::cubic_lambda(w[-3 * SY], w[-SY], w[SY], w[3 * SY], nat);
+        if (oz == 4 && oy == 4) pred = E::half(F::add(czf(), cyf()));
+        else if (oz == 4) pred = czf();
+        else pred = cyf();
       } else if (ox == 3) {
         pred = E::quad_l(p, a, b);
       } else {
         pred = E::quad_r_cube(a, b, c);
       }
-      emit_at(wi, cw0 + 2 * j + 1, true, pred);
-      p = a;
-      a = b;
-      b = c;
-      if (j + 3 <= 8) c = win[w0 + 2 * (j + 3)];
+      emit_read(w0 + 2 * j + 1, cw0 + 2 * j + 1, true, v[i], pred);
     }
   }
   // ---- level 0 of an edge tile (the last slab along some axis) by jobs ----
@@ -623,69 +697,78 @@ struct LevelSweep {
     if (o == 1) return E::lin(a, b);
     return a;
   }
-  // line_at (MD) along a runtime stride, every order
-  __device__ __forceinline__ T line_rt(const T* w, int S, int o) const {
+  // line_at (MD) along an axis given by its neighbour offsets, every order
+  __device__ __forceinline__ T line_rt(const T* w, const Nb& n, int o) const {
     using E = Expr<T>;
-    const T t1 = w[-S];
+    const T t1 = w[n.m1];
     if (o == 0) return t1;
-    const T t2 = w[S];
-    if (o == 4) return E::cubic_lambda(w[-3 * S], t1, t2, w[3 * S], nat);
-    if (o == 3) return E::quad_l(w[-3 * S], t1, t2);
-    if (o == 2) return E::quad_r(t1, t2, w[3 * S]);
+    const T t2 = w[n.p1];
+    if (o == 4) return E::cubic_lambda(w[n.m3], t1, t2, w[n.p3], nat);
+    if (o == 3) return E::quad_l(w[n.m3], t1, t2);
+    if (o == 2) return E::quad_r(t1, t2, w[n.p3]);
     return E::lin(t1, t2);
   }
+  // neighbour offsets along axis d of this level's points (odd coordinates
+  // at level 0, even ones above)
+  static __device__ __forceinline__ Nb nb(int d) { return U == 1 ? nb_odd<T>(d) : nb_even<T>(d, U); }
   // KIND 0 md lines, 2 per-axis lines, 1 md faces (J = the reference's a2,
   // K = a1, at odd coordinate ck: face_at's full case table).  Point j of a
   // job is at coordinate (2j+1)U along J; its line's even values at 2kU.
+  // w0: the slot of the line's point at coordinate 0 along J.  The line's
+  // even point k (coordinate 2kU) sits at w0 + k E2, its point j (coordinate
+  // (2j+1)U) at w0 + j E2 + P0.
   template <int KIND>
   __device__ __forceinline__ void edge_job(int w0, int J, int K, int cw0, int cs, bool own, int j0, int j1,
                                            int ck) const {
     using E = Expr<T>;
     using F = Fp<T>;
-    const int S = U * (J == 0 ? 1 : (J == 1 ? kWin : kWin * kWin));
+    const int E2 = U * Win<T>::step2(J), P0 = U == 1 ? Win<T>::one(J) : (U / 2) * Win<T>::step2(J);
     const int l3 = lim3(J), l1 = lim1(J), r = lim_r(J);
-    int SK = 0, ok = 0;
+    int ok = 0;
+    Nb nk{0, 0, 0, 0}, nj{0, 0, 0, 0};
     if (KIND == 1) {
-      SK = U * (K == 0 ? 1 : (K == 1 ? kWin : kWin * kWin));
+      nk = nb(K);
+      nj = nb(J);
       ok = order_rt(ck, lim3(K), lim1(K));
     }
-    T p = j0 > 0 ? win[w0 + 2 * (j0 - 1) * S] : T(0);
-    T a = win[w0 + 2 * j0 * S], b = win[w0 + 2 * (j0 + 1) * S];
-    T c = j0 + 2 <= N ? win[w0 + 2 * (j0 + 2) * S] : T(0);
+    T p = j0 > 0 ? win[w0 + (j0 - 1) * E2] : T(0);
+    T a = win[w0 + j0 * E2], b = win[w0 + (j0 + 1) * E2];
+    T c = j0 + 2 <= N ? win[w0 + (j0 + 2) * E2] : T(0);
 #pragma unroll 1
     for (int j = j0; j < j1 && (2 * j + 1) * U < r; ++j) {
-      const int wi = w0 + (2 * j + 1) * S;
+      const int wi = w0 + j * E2 + P0;
       const int oj = order_rt((2 * j + 1) * U, l3, l1);
       const T lj = window_line<KIND != 2>(oj, p, a, b, c);
       T pred = lj;
       if (KIND == 1) {
         if (ok == 4 || oj == 4) {
           if (ok != 4) pred = lj;
-          else if (oj != 4) pred = line_rt(win + wi, SK, ok);
-          else pred = E::half(F::add(line_rt(win + wi, SK, ok), lj));
+          else if (oj != 4) pred = line_rt(win + wi, nk, ok);
+          else pred = E::half(F::add(line_rt(win + wi, nk, ok), lj));
         } else if ((ok >= 2 && oj >= 2) || (ok == 1 && oj == 1)) {
-          pred = E::half(F::add(line_rt(win + wi, SK, ok), lj));
+          pred = E::half(F::add(line_rt(win + wi, nk, ok), lj));
         } else if (ok >= 2 || (ok == 1 && oj == 0)) {
-          pred = line_rt(win + wi, SK, ok);
+          pred = line_rt(win + wi, nk, ok);
         } else if (oj >= 1) {
           pred = lj;
         } else {
-          pred = F::sub(F::add(win[wi - SK], win[wi - S]), win[wi - SK - S]);
+          pred = F::sub(F::add(win[wi + nk.m1], win[wi + nj.m1]), win[wi + nk.m1 + nj.m1]);
         }
       }
       emit_at(wi, cw0 + (2 * j + 1) * U * cs, own, pred);
       p = a;
       a = b;
       b = c;
-      if (j + 3 <= N) c = win[w0 + 2 * (j + 3) * S];
+      if (j + 3 <= N) c = win[w0 + (j + 3) * E2];
     }
   }
   // md cube points (x odd, cy, cz) along x with cube_at's full case order
   __device__ __forceinline__ void edge_cube_job(int cy, int cz, int j0, int j1) const {
     using E = Expr<T>;
     using F = Fp<T>;
-    constexpr int SX = U, SY = U * kWin, SZ = U * kWin * kWin;
-    const int w0 = (cz * kWin + cy) * kWin, cw0 = (cz * 16 + cy) * 16;
+    constexpr int SX = U;  // x is not skewed
+    const int w0 = Win<T>::at(0, cy, cz), cw0 = (cz * 16 + cy) * 16;
+    const Nb ny = nb(1), nz = nb(2);
     const int oy = order_rt(cy, lim3(1), lim1(1)), oz = order_rt(cz, lim3(2), lim1(2));
     const int l3 = lim3(0), l1 = lim1(0), r = lim_r(0);
     T p = j0 > 0 ? win[w0 + 2 * (j0 - 1) * SX] : T(0);
@@ -696,8 +779,8 @@ struct LevelSweep {
       const int wi = w0 + (2 * j + 1) * SX;
       const T* w = win + wi;
       const int ox = order_rt((2 * j + 1) * U, l3, l1);
-      auto cy_ = [&]() { return E::cubic_lambda(w[-3 * SY], w[-SY], w[SY], w[3 * SY], nat); };
-      auto cz_ = [&]() { return E::cubic_lambda(w[-3 * SZ], w[-SZ], w[SZ], w[3 * SZ], nat); };
+      auto cy_ = [&]() { return E::cubic_lambda(w[ny.m3], w[ny.m1], w[ny.p1], w[ny.p3], nat); };
+      auto cz_ = [&]() { return E::cubic_lambda(w[nz.m3], w[nz.m1], w[nz.p1], w[nz.p3], nat); };
       auto cx_ = [&]() { return E::cubic_lambda(p, a, b, c, nat); };
       T pred;
       if (oz == 4 && oy == 4 && ox == 4) pred = F::div(F::add(F::add(cx_(), cy_()), cz_()), T(3));
@@ -718,6 +801,11 @@ struct LevelSweep {
       if (j + 3 <= N) c = win[w0 + 2 * (j + 3) * SX];
     }
   }
+  // slot of the window point with coordinate ca on axis a, cb on axis b and
+  // 0 on the third
+  static __device__ __forceinline__ int at2(int a, int ca, int b, int cb) {
+    return Win<T>::axis(a, ca) + Win<T>::axis(b, cb);
+  }
   // Level 1 (unit 2, four odd points per line) of any tile by half-line jobs
   // with the runtime orders; not the last level, so every point in the field
   // is predicted.  md: 150 line, 120 face and 32 cube jobs; per axis: 50,
@@ -725,20 +813,19 @@ struct LevelSweep {
   __device__ __forceinline__ void mid_md_jobs() const {
     static_assert(U == 2, "level 1");
     const int t = threadIdx.x;
-    auto kS = [](int a) { return a == 0 ? 1 : (a == 1 ? kWin : kWin * kWin); };
     auto kC = [](int a) { return a == 0 ? 1 : (a == 1 ? 16 : 256); };
     if (t < 150) {
       const int h = t / 75, r = t - 75 * h, f = r / 25, l = r - 25 * f, u = 4 * (l % 5), v = 4 * (l / 5);
       const int P = f == 0 ? 1 : 0, Q = f == 2 ? 1 : 2;
       if (u < lim_r(P) && v < lim_r(Q))
-        edge_job<0>(u * kS(P) + v * kS(Q), f, 0, u * kC(P) + v * kC(Q), kC(f), (u | v) < 16, 2 * h, 2 * h + 2, 0);
+        edge_job<0>(at2(P, u, Q, v), f, 0, u * kC(P) + v * kC(Q), kC(f), (u | v) < 16, 2 * h, 2 * h + 2, 0);
     }
     __syncthreads();
     if (t < 120) {
       const int h = t / 60, r = t - 60 * h, f = r / 20, l = r - 20 * f, ce = 4 * (l % 5), ck = 4 * (l / 5) + 2;
       const int J = f == 0 ? 1 : 0, K = f == 1 ? 2 : (f == 0 ? 2 : 1);
       if (ce < lim_r(f) && ck < lim_r(K))
-        edge_job<1>(ce * kS(f) + ck * kS(K), J, K, ce * kC(f) + ck * kC(K), kC(J), ce < 16, 2 * h, 2 * h + 2, ck);
+        edge_job<1>(at2(f, ce, K, ck), J, K, ce * kC(f) + ck * kC(K), kC(J), ce < 16, 2 * h, 2 * h + 2, ck);
     }
     __syncthreads();
     if (t < 32) {
@@ -749,58 +836,57 @@ struct LevelSweep {
   }
   __device__ __forceinline__ void mid_axis_jobs(bool rev) const {
     static_assert(U == 2, "level 1");
-    constexpr int SY = kWin, SZ = kWin * kWin;
+    using W = Win<T>;
     const int t = threadIdx.x;
     const int r0 = lim_r(0), r1 = lim_r(1), r2 = lim_r(2);
     if (!rev) {  // z at (x, y) even; y at (x even, z any); x at (y, z any)
       if (t < 50) {
         const int h = t / 25, l = t - 25 * h, x = 4 * (l % 5), y = 4 * (l / 5);
-        if (x < r0 && y < r1) edge_job<2>(x + y * SY, 2, 0, x + 16 * y, 256, (x | y) < 16, 2 * h, 2 * h + 2, 0);
+        if (x < r0 && y < r1) edge_job<2>(W::at(x, y, 0), 2, 0, x + 16 * y, 256, (x | y) < 16, 2 * h, 2 * h + 2, 0);
       }
       __syncthreads();
       if (t < 90) {
         const int h = t / 45, l = t - 45 * h, x = 4 * (l % 5), z = 2 * (l / 5);
-        if (x < r0 && z < r2) edge_job<2>(x + z * SZ, 1, 0, x + 256 * z, 16, (x | z) < 16, 2 * h, 2 * h + 2, 0);
+        if (x < r0 && z < r2) edge_job<2>(W::at(x, 0, z), 1, 0, x + 256 * z, 16, (x | z) < 16, 2 * h, 2 * h + 2, 0);
       }
       __syncthreads();
       if (t < 162) {
         const int h = t / 81, l = t - 81 * h, y = 2 * (l % 9), z = 2 * (l / 9);
-        if (y < r1 && z < r2) edge_job<2>(y * SY + z * SZ, 0, 0, 16 * y + 256 * z, 1, (y | z) < 16, 2 * h, 2 * h + 2, 0);
+        if (y < r1 && z < r2) edge_job<2>(W::at(0, y, z), 0, 0, 16 * y + 256 * z, 1, (y | z) < 16, 2 * h, 2 * h + 2, 0);
       }
     } else {  // x at (y, z) even; y at (x any, z even); z at (x, y any)
       if (t < 50) {
         const int h = t / 25, l = t - 25 * h, y = 4 * (l % 5), z = 4 * (l / 5);
-        if (y < r1 && z < r2) edge_job<2>(y * SY + z * SZ, 0, 0, 16 * y + 256 * z, 1, (y | z) < 16, 2 * h, 2 * h + 2, 0);
+        if (y < r1 && z < r2) edge_job<2>(W::at(0, y, z), 0, 0, 16 * y + 256 * z, 1, (y | z) < 16, 2 * h, 2 * h + 2, 0);
       }
       __syncthreads();
       if (t < 90) {
         const int h = t / 45, l = t - 45 * h, x = 2 * (l % 9), z = 4 * (l / 9);
-        if (x < r0 && z < r2) edge_job<2>(x + z * SZ, 1, 0, x + 256 * z, 16, (x | z) < 16, 2 * h, 2 * h + 2, 0);
+        if (x < r0 && z < r2) edge_job<2>(W::at(x, 0, z), 1, 0, x + 256 * z, 16, (x | z) < 16, 2 * h, 2 * h + 2, 0);
       }
       __syncthreads();
       if (t < 162) {
         const int h = t / 81, l = t - 81 * h, x = 2 * (l % 9), y = 2 * (l / 9);
-        if (x < r0 && y < r1) edge_job<2>(x + y * SY, 2, 0, x + 16 * y, 256, (x | y) < 16, 2 * h, 2 * h + 2, 0);
+        if (x < r0 && y < r1) edge_job<2>(W::at(x, y, 0), 2, 0, x + 16 * y, 256, (x | y) < 16, 2 * h, 2 * h + 2, 0);
       }
     }
     __syncthreads();
   }
   __device__ __forceinline__ void edge_md_lines() const {
     const int t = threadIdx.x;
-    auto kS = [](int a) { return a == 0 ? 1 : (a == 1 ? kWin : kWin * kWin); };
     auto kC = [](int a) { return a == 0 ? 1 : (a == 1 ? 16 : 256); };
     if (t < 243) {
       const int f = t / 81, l = t - 81 * f, u = 2 * (l % 9), v = 2 * (l / 9);
       const int P = f == 0 ? 1 : 0, Q = f == 2 ? 1 : 2;
       if (u < lim_r(P) && v < lim_r(Q))
-        edge_job<0>(u * kS(P) + v * kS(Q), f, 0, u * kC(P) + v * kC(Q), kC(f), (u | v) < 16, 0, 8, 0);
+        edge_job<0>(at2(P, u, Q, v), f, 0, u * kC(P) + v * kC(Q), kC(f), (u | v) < 16, 0, 8, 0);
     }
     __syncthreads();
     if (t < 216) {
       const int f = t / 72, l = t - 72 * f, ce = 2 * (l % 9), ck = 2 * (l / 9) + 1;
       const int J = f == 0 ? 1 : 0, K = f == 1 ? 2 : (f == 0 ? 2 : 1);
       if (ce < lim_r(f) && ck < lim_r(K))
-        edge_job<1>(ce * kS(f) + ck * kS(K), J, K, ce * kC(f) + ck * kC(K), kC(J), ce < 16, 0, 8, ck);
+        edge_job<1>(at2(f, ce, K, ck), J, K, ce * kC(f) + ck * kC(K), kC(J), ce < 16, 0, 8, ck);
     }
     __syncthreads();
     {
@@ -810,64 +896,71 @@ struct LevelSweep {
     __syncthreads();
   }
   __device__ __forceinline__ void edge_axis_lines(bool rev) const {
-    constexpr int SY = kWin, SZ = kWin * kWin;
+    using W = Win<T>;
     const int t = threadIdx.x;
     const int r0 = lim_r(0), r1 = lim_r(1), r2 = lim_r(2);
     if (!rev) {  // z, then y, then x
       if (t < 162) {
         const int l = t >> 1, x = 2 * (l % 9), y = 2 * (l / 9), j0 = (t & 1) * 4;
-        if (x < r0 && y < r1) edge_job<2>(x + y * SY, 2, 0, x + 16 * y, 256, (x | y) < 16, j0, j0 + 4, 0);
+        if (x < r0 && y < r1) edge_job<2>(W::at(x, y, 0), 2, 0, x + 16 * y, 256, (x | y) < 16, j0, j0 + 4, 0);
       }
       __syncthreads();
       if (t < 144) {
         const int x = 2 * (t % 9), z = t / 9;
-        if (x < r0 && z < r2) edge_job<2>(x + z * SZ, 1, 0, x + 256 * z, 16, x < 16, 0, 8, 0);
+        if (x < r0 && z < r2) edge_job<2>(W::at(x, 0, z), 1, 0, x + 256 * z, 16, x < 16, 0, 8, 0);
       }
       __syncthreads();
       const int y = t & 15, z = t >> 4;
-      if (y < r1 && z < r2) edge_job<2>(y * SY + z * SZ, 0, 0, 16 * y + 256 * z, 1, true, 0, 8, 0);
+      if (y < r1 && z < r2) edge_job<2>(W::at(0, y, z), 0, 0, 16 * y + 256 * z, 1, true, 0, 8, 0);
     } else {  // x, then y, then z
       if (t < 162) {
         const int l = t >> 1, y = 2 * (l % 9), z = 2 * (l / 9), j0 = (t & 1) * 4;
-        if (y < r1 && z < r2) edge_job<2>(y * SY + z * SZ, 0, 0, 16 * y + 256 * z, 1, (y | z) < 16, j0, j0 + 4, 0);
+        if (y < r1 && z < r2) edge_job<2>(W::at(0, y, z), 0, 0, 16 * y + 256 * z, 1, (y | z) < 16, j0, j0 + 4, 0);
       }
       __syncthreads();
       if (t < 144) {
         const int x = t & 15, z = 2 * (t >> 4);
-        if (x < r0 && z < r2) edge_job<2>(x + z * SZ, 1, 0, x + 256 * z, 16, z < 16, 0, 8, 0);
+        if (x < r0 && z < r2) edge_job<2>(W::at(x, 0, z), 1, 0, x + 256 * z, 16, z < 16, 0, 8, 0);
       }
       __syncthreads();
       const int x = t & 15, y = t >> 4;
-      if (x < r0 && y < r1) edge_job<2>(x + y * SY, 2, 0, x + 16 * y, 256, true, 0, 8, 0);
+      if (x < r0 && y < r1) edge_job<2>(W::at(x, y, 0), 2, 0, x + 16 * y, 256, true, 0, 8, 0);
     }
     __syncthreads();
   }
+  // Stage-to-lane maps of the interior md level 0, chosen with the window
+  // layout (Win) to spread each warp's accesses over the banks: a face
+  // family whose bit is set in kFaceSwap takes its jobs with the odd
+  // coordinate fastest; the cube's quarter-line jobs go line-fastest, with y
+  // (double) or z (float) fastest across the lines.
+  static constexpr int kFaceSwap = sizeof(T) == 8 ? 6 : 4;
   // md level 0: lines (243 jobs), faces (216 jobs), cube (256 quarter-line
   // jobs), one barrier per stage
   __device__ __forceinline__ void level0_md_lines() const {
     static_assert(kPredThreads == 256, "one cube quarter-line per thread");
     const int t = threadIdx.x;
-    auto kS = [](int a) { return a == 0 ? 1 : (a == 1 ? kWin : kWin * kWin); };  // window stride
-    auto kC = [](int a) { return a == 0 ? 1 : (a == 1 ? 16 : 256); };          // code-block stride
+    auto kC = [](int a) { return a == 0 ? 1 : (a == 1 ? 16 : 256); };  // code-block stride
     if (t < 243) {
       // family f: lines along axis f through the other two (even) coordinates
       const int f = t / 81, l = t - 81 * f, u = 2 * (l % 9), v = 2 * (l / 9);
       const int P = f == 0 ? 1 : 0, Q = f == 2 ? 1 : 2;  // the fixed axes
-      const int w0 = u * kS(P) + v * kS(Q);
-      md_job<0>(w0, kS(f), u * kC(P) + v * kC(Q), kC(f), (u | v) < 16, 0, 8, 0, 0);
+      md_job<0>(at2(P, u, Q, v), f, u * kC(P) + v * kC(Q), kC(f), (u | v) < 16, 0, 8, 0, 0);
     }
     __syncthreads();
     if (t < 216) {
       // family f: the even axis EA = f; jobs along J, second odd axis K
-      const int f = t / 72, l = t - 72 * f, ce = 2 * (l % 9), ck = 2 * (l / 9) + 1;
+      const int f = t / 72, l = t - 72 * f;
+      const bool swap = (kFaceSwap >> f) & 1;
+      const int ce = swap ? 2 * (l >> 3) : 2 * (l % 9), ck = swap ? 2 * (l & 7) + 1 : 2 * (l / 9) + 1;
       const int J = f == 0 ? 1 : 0, K = f == 1 ? 2 : (f == 0 ? 2 : 1);
-      const int w0 = ce * kS(f) + ck * kS(K);
-      md_job<1>(w0, kS(J), ce * kC(f) + ck * kC(K), kC(J), ce < 16, 0, 8, kS(K), order0(ck));
+      md_job<1>(at2(f, ce, K, ck), J, ce * kC(f) + ck * kC(K), kC(J), ce < 16, 0, 8, K, order0(ck));
     }
     __syncthreads();
     {
-      const int line = t >> 2, q = t & 3;
-      md_cube_job(2 * (line & 7) + 1, 2 * (line >> 3) + 1, 2 * q, 2 * q + 2);
+      const int line = t & 63, q = t >> 6;
+      const int a = 2 * (line & 7) + 1, b = 2 * (line >> 3) + 1;
+      if (sizeof(T) == 8) md_cube_job(b, a, 2 * q);
+      else md_cube_job(a, b, 2 * q);
     }
     __syncthreads();
   }
@@ -879,34 +972,34 @@ struct LevelSweep {
   // lines; last stage: the tile's 256 lines, one per thread.
   __device__ __forceinline__ void level0_lines(bool rev) const {
     static_assert(kPredThreads == 256, "one last-stage line per thread");
-    constexpr int SY = kWin, SZ = kWin * kWin;
+    using W = Win<T>;
     const int t = threadIdx.x;
     if (!rev) {  // z, then y, then x
       if (t < 162) {
         const int l = t >> 1, x = 2 * (l % 9), y = 2 * (l / 9), j0 = (t & 1) * 4;
-        md_job<2>(x + y * SY, SZ, x + 16 * y, 256, (x | y) < 16, j0, j0 + 4, 0, 0);
+        md_job<2>(W::at(x, y, 0), 2, x + 16 * y, 256, (x | y) < 16, j0, j0 + 4, 0, 0);
       }
       __syncthreads();
       if (t < 144) {
         const int x = 2 * (t % 9), z = t / 9;
-        md_job<2>(x + z * SZ, SY, x + 256 * z, 16, x < 16, 0, 8, 0, 0);
+        md_job<2>(W::at(x, 0, z), 1, x + 256 * z, 16, x < 16, 0, 8, 0, 0);
       }
       __syncthreads();
       const int y = t & 15, z = t >> 4;
-      md_job<2>(y * SY + z * SZ, 1, 16 * y + 256 * z, 1, true, 0, 8, 0, 0);
+      md_job<2>(W::at(0, y, z), 0, 16 * y + 256 * z, 1, true, 0, 8, 0, 0);
     } else {  // x, then y, then z
       if (t < 162) {
         const int l = t >> 1, y = 2 * (l % 9), z = 2 * (l / 9), j0 = (t & 1) * 4;
-        md_job<2>(y * SY + z * SZ, 1, 16 * y + 256 * z, 1, (y | z) < 16, j0, j0 + 4, 0, 0);
+        md_job<2>(W::at(0, y, z), 0, 16 * y + 256 * z, 1, (y | z) < 16, j0, j0 + 4, 0, 0);
       }
       __syncthreads();
       if (t < 144) {
         const int x = t & 15, z = 2 * (t >> 4);
-        md_job<2>(x + z * SZ, SY, x + 256 * z, 16, z < 16, 0, 8, 0, 0);
+        md_job<2>(W::at(x, 0, z), 1, x + 256 * z, 16, z < 16, 0, 8, 0, 0);
       }
       __syncthreads();
       const int x = t & 15, y = t >> 4;
-      md_job<2>(x + y * SY, SZ, x + 16 * y, 256, true, 0, 8, 0, 0);
+      md_job<2>(W::at(x, y, 0), 2, x + 16 * y, 256, true, 0, 8, 0, 0);
     }
     __syncthreads();
   }
@@ -928,7 +1021,7 @@ struct LevelSweep {
         else level0_lines(rev);
       }
       return;
-    }
+    } else {
     if (md) {
       // lines (xyzmap_line): x-lines vary y fastest, y- and z-lines vary x.
       // Points of one stage only read coarser points, so the three groups
@@ -956,6 +1049,7 @@ struct LevelSweep {
       // x: (x odd, y any, z any), vary y
       sweep<0, false, 1 | (0 << 2) | (2 << 4), 2 * N + 1, 1, 0, N, 2, 1, 2 * N + 1, 1, 0>(kLast);
     }
+    }
   }
 };
 
@@ -981,12 +1075,13 @@ __device__ void sweep_fine(T* win, int32_t* cw, const AxisLimits& lim, bool zlas
   sweep_level<T, COMPRESS, EDGE, 1, 0>(win, cw, lim, zlast, p);
 }
 
-// window index of the j-th of the 9^3 points with all coordinates even
+// window slot of the j-th of the 9^3 points with all coordinates even
+template <class T>
 __device__ __forceinline__ int even_point(int j, int& x, int& y, int& z) {
   x = 2 * (j % 9);
   y = 2 * ((j / 9) % 9);
   z = 2 * (j / 81);
-  return (z * kWin + y) * kWin + x;
+  return Win<T>::at(x, y, z);
 }
 
 // ---- tiles -------------------------------------------------------------------
@@ -1093,25 +1188,26 @@ __device__ __forceinline__ uint64_t slot_of(const uint64_t* rows, int lv, int x,
 }
 
 // Shared memory of a compression tile: the value window and the codes of the
-// tile's own points (~55 KB for double, so four tiles fit an SM; ~36 KB for
-// float).  The row table takes the window's place once the sweeps are done.
+// tile's own points (~56 KB for double, so four tiles fit an SM; ~36 KB for
+// float, six).  The row table takes the window's place once the sweeps are
+// done.
 template <class T>
 struct CompressSmem {
-  T win[kWinVol];  // after the sweeps: the row table
+  T win[Win<T>::kSize];  // after the sweeps: the row table
   int32_t cw[16 * 16 * 16];  // codes of the tile's own points
   PredParams<T> p;
 };
-static_assert(sizeof(float) * kWinVol >= sizeof(uint64_t) * kRowTable, "row table fits the window");
+static_assert(sizeof(float) * Win<float>::kSize >= sizeof(uint64_t) * kRowTable, "row table fits the window");
 
 template <class T> struct PairOf;
 template <> struct PairOf<double> { using type = double2; };
 template <> struct PairOf<float> { using type = float2; };
 
 // Shared memory of a reconstruction tile: the window (codes travel in the
-// window slots) and the row table (~43 KB for double, ~23 KB for float).
+// window slots) and the row table (~44 KB for double, ~24 KB for float).
 template <class T>
 struct ReconSmem {
-  T win[kWinVol];
+  T win[Win<T>::kSize];
   uint64_t rows[kRowTable];
   PredParams<T> p;
 };
@@ -1138,7 +1234,7 @@ __device__ __forceinline__ void compress_tile(CompressSmem<T>& sm, const T* __re
   // arrive while those levels run
   for (int j = tid; j < 729; j += kPredThreads) {
     int x, y, z;
-    const int i = even_point(j, x, y, z);
+    const int i = even_point<T>(j, x, y, z);
     if (L.in_data(x, y, z)) copy_async<sizeof(T)>(&sm.win[i], base + x + (uint64_t)y * sy + (uint64_t)z * sz);
     else sm.win[i] = T(0);
   }
@@ -1148,8 +1244,9 @@ __device__ __forceinline__ void compress_tile(CompressSmem<T>& sm, const T* __re
     int x, y, z;
     win_xyz(i, x, y, z);
     if (((x | y | z) & 1) == 0) continue;
-    if (L.in_data(x, y, z)) copy_async<sizeof(T)>(&sm.win[i], base + x + (uint64_t)y * sy + (uint64_t)z * sz);
-    else sm.win[i] = T(0);
+    T* dst = &sm.win[Win<T>::at(x, y, z)];
+    if (L.in_data(x, y, z)) copy_async<sizeof(T)>(dst, base + x + (uint64_t)y * sy + (uint64_t)z * sz);
+    else *dst = T(0);
   }
   copy_async_commit();
   copy_async_wait_group<1>();
@@ -1200,6 +1297,7 @@ predict_compress_kernel(const T* __restrict__ data, Geometry g, const PredParams
 template <class T, int PART>
 constexpr int reconstruct_min_ctas() { return PART == 0 ? (sizeof(T) == 4 ? 7 : 5) : 4; }
 
+
 template <class T, bool PROG, int PART>
 __global__ void __launch_bounds__(kPredThreads, reconstruct_min_ctas<T, PART>())
 reconstruct_kernel(const int32_t* __restrict__ qc, const T* __restrict__ anchors, Geometry g,
@@ -1235,7 +1333,7 @@ reconstruct_kernel(const int32_t* __restrict__ qc, const T* __restrict__ anchors
   // level-0 codes, which arrive while levels 3..1 run.
   for (int j = tid; j < 729; j += kPredThreads) {
     int x, y, z;
-    const int i = even_point(j, x, y, z);
+    const int i = even_point<T>(j, x, y, z);
     const int lv = win_level(x, y, z);
     int32_t* dst = reinterpret_cast<int32_t*>(&sm.win[i]);
     if (lv < 4 && lv <= maxlevel && L.in_data(x, y, z)) copy_async<4>(dst, qc + slot_of(sm.rows, lv, x, y, z));
@@ -1252,14 +1350,14 @@ reconstruct_kernel(const int32_t* __restrict__ qc, const T* __restrict__ anchors
       const int y = r % kWin, z = r / kWin;
       const int ee = ((y | z) & 1) == 0;
       if (ee && !(x & 1)) continue;
-      T* dst = &sm.win[r * kWin + x];
+      T* dst = &sm.win[Win<T>::at(x, y, z)];
       if (maxlevel >= 0 && L.in_data(x, y, z)) copy_async<4>(dst, qc + (sm.rows[r] + (uint64_t)(x >> ee)));
       else *dst = T(0);
     }
     for (int r = tid; r < kWin * kWin; r += kPredThreads) {
       const int y = r % kWin, z = r / kWin;
       if (((y | z) & 1) == 0) continue;
-      T* dst = &sm.win[r * kWin + 16];
+      T* dst = &sm.win[Win<T>::at(16, y, z)];
       if (maxlevel >= 0 && L.in_data(16, y, z)) copy_async<4>(dst, qc + (sm.rows[r] + 16));
       else *dst = T(0);
     }
@@ -1271,7 +1369,7 @@ reconstruct_kernel(const int32_t* __restrict__ qc, const T* __restrict__ anchors
     int x = (tid & 1) * 16, y = ((tid >> 1) & 1) * 16, z = (tid >> 2) * 16;
     uint32_t ax = x / 16 + bi[0], ay = y / 16 + bi[1], az = z / 16 + bi[2];
     if (ax < g.ax && ay < g.ay && az < g.az)
-      sm.win[(z * kWin + y) * kWin + x] = anchors[ax + (uint64_t)ay * g.ax + (uint64_t)az * g.ax * g.ay];
+      sm.win[Win<T>::at(x, y, z)] = anchors[ax + (uint64_t)ay * g.ax + (uint64_t)az * g.ax * g.ay];
   }
   __syncthreads();
   sweep_coarse<T, false, EDGE>(sm.win, nullptr, f.lim, f.last[2], sm.p);
@@ -1299,7 +1397,7 @@ reconstruct_kernel(const int32_t* __restrict__ qc, const T* __restrict__ anchors
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
           const int q = b + k * kPredThreads, x = 2 * (q & 7), y = (q >> 3) & 15, z = q >> 7;
-          const int wi = (z * kWin + y) * kWin + x;
+          const int wi = Win<T>::at(x, y, z);
           V v;
           v.x = sm.win[wi];
           v.y = sm.win[wi + 1];
@@ -1331,7 +1429,7 @@ reconstruct_kernel(const int32_t* __restrict__ qc, const T* __restrict__ anchors
       int i = b + k * kPredThreads;
       int x = i % xs, y = (i / xs) % ys, z = i / (xs * ys);
       if (i >= total || !L.in_data(x, y, z)) continue;
-      T v = sm.win[(z * kWin + y) * kWin + x];
+      T v = sm.win[Win<T>::at(x, y, z)];
       out[base + x + (uint64_t)y * sy + (uint64_t)z * sz] = PROG ? Fp<T>::add(v, o[k]) : v;
     }
   }

@@ -65,6 +65,7 @@ struct Small {
   StrategyBest sblk[kStrategyCells];
   double errors[16];
   double minmax[2];
+  int dec_begin[4];  // progressive exact mode: the first plane whose chunks a step decodes, per level
 };
 
 struct HostResult {
@@ -223,6 +224,7 @@ struct prism_prog {
   uint64_t loaded = 0;          // host copy, valid when !pending
   cudaEvent_t done = nullptr;   // recorded after the last enqueued step
   bool pending = false;
+  bool exact = false;           // later steps decode the chunks of plane begin - 1 as well
 };
 
 static int fail(prism_handle* h, int code, const char* what, cudaError_t e = cudaSuccess) {
@@ -280,7 +282,7 @@ static cudaError_t smem_limit(int bytes) {
 }
 
 // The tile kernels run as two launches: interior tiles (part 0) and the tiles
-// on the field's last slabs (part 1).
+// on the field's last slabs (part 1), on two streams.
 template <class T>
 static int launch_predict(prism_handle* h, const T* in, const Geometry& g, const PredParams<T>* pp, T* anchors,
                           int32_t* qc, cudaStream_t st) {
@@ -846,15 +848,24 @@ int prism_progressive_open(prism_handle* h, const void* d_container, uint64_t si
   return PRISM_OK;
 }
 
-// strategy_finish_kernel + params_kernel of a progressive step in one launch
+// strategy_finish_kernel + params_kernel of a progressive step in one launch.
+// dec_begin (exact mode, may be null): per level, the first plane whose
+// chunks the step decodes: begin - 1 where the level has a plane below the
+// step's range and planes in it, else begin.
 template <class T>
 __global__ void prog_plan_kernel(const StrategyBest* __restrict__ blk, int mode, double bound, double target,
                                  const double* __restrict__ range, StrategyState* st, double alpha,
-                                 const uint8_t* __restrict__ flags, PredParams<T>* params, double* eb_out) {
+                                 const uint8_t* __restrict__ flags, PredParams<T>* params, double* eb_out,
+                                 int* dec_begin) {
   strategy_finish_warp(blk, mode, bound, target, range, st);
   if (threadIdx.x != 0) return;
   compute_params<T>(mode, bound, range, alpha, nullptr, 0, flags, 4, params, nullptr, eb_out);
   params->maxlevel = st->maxlevel;
+  if (dec_begin)
+    for (int i = 0; i < 4; ++i) {
+      const int b = st->begin[i];
+      dec_begin[i] = b > 0 && b < st->end[i] ? b - 1 : b;
+    }
 }
 
 __global__ void prog_init_kernel(StrategyState* st, int* err) {
@@ -919,7 +930,8 @@ static int progressive_step_t(prism_prog* p, double target, const T* prev, T* va
   // the strategy's plane ranges, then the parameters with its maxlevel
   prog_plan_kernel<T><<<1, 32, 0, st>>>(s->sblk, p->mode, p->bound, target, range, ds,
                                         alpha_of(p->mode == 1 ? p->bound : 0.0), tr,
-                                        reinterpret_cast<PredParams<T>*>(s->params), &s->eb);
+                                        reinterpret_cast<PredParams<T>*>(s->params), &s->eb,
+                                        p->exact ? s->dec_begin : nullptr);
   prof_end(h, kStStrategy, st);
   h->launches += 2;
   // chunk offsets: once per object when it holds a slot
@@ -933,9 +945,10 @@ static int progressive_step_t(prism_prog* p, double target, const T* prev, T* va
     }
     offs = ob.as<int64_t>();
   }
-  // chunks of planes the step does not load are written as zeros
-  rc = launch_decode(h, p->cont, p->size - g.header_size, g, ds->begin, ds->end, h->planes.as<uint8_t>(), st,
-                     p->d_err, offs);
+  // chunks of planes the step does not load are written as zeros; the
+  // inverse shuffle keeps planes [begin, end) of what was decoded
+  rc = launch_decode(h, p->cont, p->size - g.header_size, g, p->exact ? s->dec_begin : ds->begin, ds->end,
+                     h->planes.as<uint8_t>(), st, p->d_err, offs);
   if (rc) return rc;
   rc = launch_inverse(h, h->planes.as<uint8_t>(), g, 1 /*NB*/, ds->begin, ds->end, h->qc.as<int32_t>(), st);
   if (rc) return rc;
@@ -1006,6 +1019,12 @@ int prism_progressive_resume(prism_prog* p, const int end[4], void* stream) {
   for (int i = 0; i < 4; ++i) p->state.begin[i] = p->state.end[i] = end[i];
   p->state.maxlevel = 4;
   p->steps = 1;  // the next step adds to previous values, from zero anchors
+  return PRISM_OK;
+}
+
+int prism_progressive_exact(prism_prog* p, int enable) {
+  if (!p) return PRISM_ERR_ARG;
+  p->exact = enable != 0;
   return PRISM_OK;
 }
 

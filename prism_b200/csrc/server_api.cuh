@@ -7,12 +7,15 @@
 // plane selection that t calls for (the strategy from no planes): either in
 // one step from no planes (strategy, decode of the selected planes, inverse
 // shuffle, reconstruction), or -- when a reconstruction of f with a coarser
-// selection is resident -- as the reference's refinement step from that
-// entry (src/prism.cu:126-138: output_old -> output_new, only the planes the
-// entry lacks are decoded and their delta added).  Both carry the same
-// planes; they differ only by the floating-point rounding of the refinement
-// sum.  Reconstructions are cached per (field, selected planes): a request
-// whose selection is cached or being computed is served from that entry.
+// selection is resident -- as a refinement step from that entry
+// (src/prism.cu:126-138: output_old -> output_new, only the planes the entry
+// lacks are decoded and their delta added) in exact mode
+// (prism_progressive_exact: the reference's own refinement step misses the
+// head of the first new plane and can end far from the one-step result).
+// Both carry the same planes; they differ only by the floating-point
+// rounding of the refinement sum.  Reconstructions are cached per (field,
+// selected planes): a request whose selection is cached or being computed is
+// served from that entry.
 //
 // Continuous batching: `slots` worker threads, each with its own stream and
 // workspace, pull requests from one queue; a request is admitted when a slot
@@ -219,6 +222,7 @@ void srv_worker(prism_server* s, int slot) {
           rc = cudaMallocAsync(&p, f.value_bytes, st) == cudaSuccess ? PRISM_OK : PRISM_ERR_NOMEM;
           prism_prog* pg = nullptr;
           if (!rc) rc = prism_progressive_open(h, f.d_cont, f.size, f.tsize, f.nx, f.ny, f.nz, f.mode, f.bound, &pg);
+          if (!rc && base) rc = prism_progressive_exact(pg, 1);
           if (!rc && base) rc = prism_progressive_resume(pg, base_end, st);
           if (!rc) rc = base ? prism_progressive_step_into(pg, r->target, base_values, p, st)
                              : prism_progressive_step(pg, r->target, p, st);

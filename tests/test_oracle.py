@@ -136,3 +136,26 @@ def test_oracle_predictor_bound_every_shape():
                 old = np.ones(shape, dtype=dtype)
                 prog = O.reconstruct(qc, anchors, shape, dtype, 1e-3, md, rv, 0.0, 4, old)
                 assert np.array_equal(prog, (out + old).astype(dtype))
+
+
+def test_exact_refinement_equals_one_step():
+    """The oracle's exact refinement (the chunks of plane begin - 1 decoded
+    as well) ends every chain within a few ulps of the one-step retrieval to
+    the same planes, while the reference's chain 1e-2 -> 1e-4 on a double
+    field with 8-byte-multiple planes misses the head of the first new plane
+    and ends far outside the 1e-4 bound."""
+    from prism_b200 import fields
+    data = fields.make("grf", (40, 48, 64), np.float64, 30)
+    shape, rng = data.shape, float(data.max() - data.min())
+    cont, _, _ = O.compress(data, 1, 1e-6, 0)
+    ulp = float(np.spacing(np.abs(data).max()))
+    one, _ = O.progressive_step(cont, shape, np.float64, 1, 1e-6, 1e-4, O.ProgressiveState())
+    for exact in (False, True):
+        st = O.ProgressiveState()
+        O.progressive_step(cont, shape, np.float64, 1, 1e-6, 1e-2, st, exact=exact)
+        two, (b, e, ml) = O.progressive_step(cont, shape, np.float64, 1, 1e-6, 1e-4, st, exact=exact)
+        d = np.abs(two - one).max()
+        if exact:
+            assert d <= 16 * ulp and np.abs(two - data).max() <= 1e-4 * rng
+        else:
+            assert d > 1e-3 * rng and np.abs(two - data).max() > 1e-3 * rng
