@@ -1135,9 +1135,6 @@ __device__ __forceinline__ void tile_frame(const G& g, const uint32_t bi[3], Til
   }
 }
 
-__device__ __forceinline__ void win_xyz(int i, int& x, int& y, int& z) {
-  x = i % kWin; y = (i / kWin) % kWin; z = i / (kWin * kWin);
-}
 
 // level of a window point: 0..3, or 4 for the stride-16 anchors (the window
 // starts on a multiple of 16, so window and global coordinates agree mod 16)
@@ -1239,14 +1236,35 @@ __device__ __forceinline__ void compress_tile(CompressSmem<T>& sm, const T* __re
     else sm.win[i] = T(0);
   }
   copy_async_commit();
-#pragma unroll 4
-  for (int i = tid; i < kWinVol; i += kPredThreads) {
-    int x, y, z;
-    win_xyz(i, x, y, z);
-    if (((x | y | z) & 1) == 0) continue;
-    T* dst = &sm.win[Win<T>::at(x, y, z)];
-    if (L.in_data(x, y, z)) copy_async<sizeof(T)>(dst, base + x + (uint64_t)y * sy + (uint64_t)z * sz);
-    else *dst = T(0);
+  // the rest by window rows r = 17 z + y: a half-warp takes x = 0..15 of a
+  // row (rows advance by 16), then a thread per row takes x = 16
+  {
+    static_assert(2 * (kPredThreads / 32) == 16, "rows advance by 16: (y, z) -> (y - 1, z + 1) or (16, z)");
+    const int lane = tid & 31, x = lane & 15;
+    int r = (tid >> 5) * 2 + (lane >> 4), y = r, z = 0;
+    const T* src = base + x + (uint64_t)y * sy;
+    for (; r < kWin * kWin; r += 16) {
+      if (((x | y | z) & 1) != 0) {
+        T* dst = &sm.win[Win<T>::at(x, y, z)];
+        if (L.in_data(x, y, z)) copy_async<sizeof(T)>(dst, src);
+        else *dst = T(0);
+      }
+      if (y == 0) {
+        y = 16;
+        src += 16 * sy;
+      } else {
+        --y;
+        ++z;
+        src += sz - sy;
+      }
+    }
+    for (int q = tid; q < kWin * kWin; q += kPredThreads) {
+      const int yq = q % kWin, zq = q / kWin;
+      if (((yq | zq) & 1) == 0) continue;  // (16, even, even): an even point
+      T* dst = &sm.win[Win<T>::at(16, yq, zq)];
+      if (L.in_data(16, yq, zq)) copy_async<sizeof(T)>(dst, base + 16 + (uint64_t)yq * sy + (uint64_t)zq * sz);
+      else *dst = T(0);
+    }
   }
   copy_async_commit();
   copy_async_wait_group<1>();
@@ -1345,14 +1363,23 @@ reconstruct_kernel(const int32_t* __restrict__ qc, const T* __restrict__ anchors
   // its 8 odd-x points at rows[r] + x/2.  Each half-warp takes x = 0..15 of
   // one row (the row's slot base is one shared broadcast), then x = 16.
   {
+    static_assert(2 * (kPredThreads / 32) == 16, "rows advance by 16: (y, z) -> (y - 1, z + 1) or (16, z)");
     const int lane = tid & 31, x = lane & 15;
-    for (int r = (tid >> 5) * 2 + (lane >> 4); r < kWin * kWin; r += 2 * (kPredThreads / 32)) {
-      const int y = r % kWin, z = r / kWin;
+    const bool codes = maxlevel >= 0;
+    int r = (tid >> 5) * 2 + (lane >> 4), y = r, z = 0;  // r = 17 z + y
+    for (; r < kWin * kWin; r += 16) {
       const int ee = ((y | z) & 1) == 0;
-      if (ee && !(x & 1)) continue;
-      T* dst = &sm.win[Win<T>::at(x, y, z)];
-      if (maxlevel >= 0 && L.in_data(x, y, z)) copy_async<4>(dst, qc + (sm.rows[r] + (uint64_t)(x >> ee)));
-      else *dst = T(0);
+      if (!ee || (x & 1)) {
+        T* dst = &sm.win[Win<T>::at(x, y, z)];
+        if (codes && L.in_data(x, y, z)) copy_async<4>(dst, qc + (sm.rows[r] + (uint64_t)(x >> ee)));
+        else *dst = T(0);
+      }
+      if (y == 0) {
+        y = 16;
+      } else {
+        --y;
+        ++z;
+      }
     }
     for (int r = tid; r < kWin * kWin; r += kPredThreads) {
       const int y = r % kWin, z = r / kWin;
