@@ -133,6 +133,17 @@ __device__ __forceinline__ Nb nb_even(int d, int u) {
   return {-3 * s, -s, s, 3 * s};
 }
 
+// Word of the compression tile's code block (16^3 int32) that holds the code
+// of own point i = x + 16 y + 256 z: x XOR a function of the row.  A stage's
+// lanes write the same x of different rows, which in the plain layout (row
+// pitch 16 words) falls into one or two banks; the row-dependent XOR (a
+// permutation within each row, so the block keeps its size) spreads them,
+// and a row still reads out as 16 distinct banks.
+__device__ __forceinline__ int cw_word(int i) {
+  const int y = (i >> 4) & 15, z = i >> 8;
+  return i ^ ((z + 2 * (y >> 1) + 3 * (z >> 1)) & 15);
+}
+
 // FAST marks an interior tile: its whole 17^3 window lies inside the field and
 // it is not the last tile along any axis, so every boundary test below folds
 // to a constant.  Both forms evaluate the same expressions on the same values.
@@ -456,7 +467,7 @@ struct LevelSweep {
     if (COMPRESS) {
       T rec;
       const int32_t code = quantize(win[wi], pred, ebr, ebx2, &rec);
-      if ((c[0] | c[1] | c[2]) < 16) cw[(c[2] * 16 + c[1]) * 16 + c[0]] = code;
+      if ((c[0] | c[1] | c[2]) < 16) cw[cw_word((c[2] * 16 + c[1]) * 16 + c[0])] = code;
       win[wi] = rec;
     } else {
       win[wi] = Fp<T>::fma(code_of(wi), ebx2, pred);
@@ -543,7 +554,7 @@ struct LevelSweep {
     if (COMPRESS) {
       T rec;
       const int32_t code = quantize(win[wi], pred, ebr, ebx2, &rec);
-      if (own) cw[cwi] = code;
+      if (own) cw[cw_word(cwi)] = code;
       win[wi] = rec;
     } else {
       win[wi] = Fp<T>::fma(code_of(wi), ebx2, pred);
@@ -555,7 +566,7 @@ struct LevelSweep {
     if (COMPRESS) {
       T rec;
       const int32_t code = quantize(v, pred, ebr, ebx2, &rec);
-      if (own) cw[cwi] = code;
+      if (own) cw[cw_word(cwi)] = code;
       win[wi] = rec;
     } else {
       win[wi] = Fp<T>::fma(v, ebx2, pred);
@@ -1191,7 +1202,7 @@ __device__ __forceinline__ uint64_t slot_of(const uint64_t* rows, int lv, int x,
 template <class T>
 struct CompressSmem {
   T win[Win<T>::kSize];  // after the sweeps: the row table
-  int32_t cw[16 * 16 * 16];  // codes of the tile's own points
+  int32_t cw[16 * 16 * 16];  // codes of the tile's own points (cw_word order)
   PredParams<T> p;
 };
 static_assert(sizeof(float) * Win<float>::kSize >= sizeof(uint64_t) * kRowTable, "row table fits the window");
@@ -1284,7 +1295,7 @@ __device__ __forceinline__ void compress_tile(CompressSmem<T>& sm, const T* __re
     const int x = i & 15, y = (i >> 4) & 15, z = i >> 8;
     const int lv = win_level(x, y, z);
     if (lv == 4 || !L.in_data(x, y, z)) continue;
-    qc[slot_of(rows, lv, x, y, z)] = sm.cw[i];
+    qc[slot_of(rows, lv, x, y, z)] = sm.cw[cw_word(i)];
   }
 }
 
