@@ -66,6 +66,7 @@ struct Small {
   double errors[16];
   double minmax[2];
   int dec_begin[4];  // progressive exact mode: the first plane whose chunks a step decodes, per level
+  unsigned char params_odd[256];  // parameters of odd progressive steps (even steps: params)
 };
 
 struct HostResult {
@@ -112,6 +113,17 @@ struct prism_handle {
   // launch (the two write disjoint tiles)
   cudaStream_t side = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
+  // Progressive steps run their strategy, plan and decode on `dec` so that a
+  // step's decode overlaps the previous step's reconstruction: the decode
+  // needs only the plane buffer, which the previous inverse shuffle (event
+  // planes_free) has consumed.  epoch counts the calls that use the handle's
+  // buffers; a step takes the short wait only when the previous such call
+  // was the previous step of the same object on the same stream.
+  cudaStream_t dec = nullptr;
+  cudaEvent_t dec_call = nullptr, dec_done = nullptr, planes_free = nullptr;
+  uint64_t epoch = 0, chain_epoch = 0;
+  const void* chain_prog = nullptr;
+  cudaStream_t chain_stream = nullptr;
   // device state slots of the progressive objects opened on this handle
   // (no allocation per open); bit i of prog_used = slot i taken
   DevBuf prog_slots;
@@ -261,7 +273,10 @@ static uint64_t qc_len(const Geometry& g) {
   return g.anchors + (uint64_t)std::max(end0, last) + 64;
 }
 
-static Small* small(prism_handle* h) { return h->small.as<Small>(); }
+static Small* small(prism_handle* h) {
+  ++h->epoch;
+  return h->small.as<Small>();
+}
 
 // Raise a kernel's dynamic shared-memory limit, once per device.
 template <auto Kernel>
@@ -317,6 +332,7 @@ static int launch_reconstruct(prism_handle* h, const int32_t* qc, const T* ancho
 }
 
 static int ensure_common(prism_handle* h, const Geometry& g) {
+  ++h->epoch;
   CKA(h->qc.ensure(qc_len(g) * sizeof(int32_t)));
   CKA(h->planes.ensure(g.aligned_size + 64));
   CKA(h->status.ensure((size_t)g.chunks * sizeof(unsigned long long)));
@@ -669,6 +685,9 @@ void prism_destroy(prism_handle* h) {
   if (h->side) cudaStreamDestroy(h->side);
   if (h->fork) cudaEventDestroy(h->fork);
   if (h->join) cudaEventDestroy(h->join);
+  if (h->dec) cudaStreamDestroy(h->dec);
+  for (cudaEvent_t e : {h->dec_call, h->dec_done, h->planes_free})
+    if (e) cudaEventDestroy(e);
   if (h->host) cudaFreeHost(h->host);
   if (h->prog_host) cudaFreeHost(h->prog_host);
   delete h;
@@ -904,6 +923,27 @@ template <class T>
 static int progressive_step_t(prism_prog* p, double target, const T* prev, T* values, cudaStream_t st) {
   prism_handle* h = p->h;
   const Geometry& g = p->g;
+  // the next step of the same object on the same stream, with no other call
+  // on the handle in between (and no stage but the reconstruction timed:
+  // per-stage timing runs the stages one after the other)
+  const bool chained = p->steps > 0 && h->chain_prog == p && h->chain_stream == st &&
+                       h->chain_epoch == h->epoch && (h->prof & ~(1u << kStReconstruct)) == 0;
+  if (!h->dec) {
+    // default priority: the step's strategy and decode CTAs fill the slots
+    // the previous reconstruction's last wave leaves idle (a high-priority
+    // stream took slots from its full waves instead, measured no faster)
+    CK(cudaStreamCreateWithFlags(&h->dec, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&h->dec_call, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&h->dec_done, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&h->planes_free, cudaEventDisableTiming));
+  }
+  cudaStream_t dst = h->dec;
+  if (chained) {
+    CK(cudaStreamWaitEvent(dst, h->planes_free, 0));
+  } else {
+    CK(cudaEventRecord(h->dec_call, st));
+    CK(cudaStreamWaitEvent(dst, h->dec_call, 0));
+  }
   int rc = ensure_common(h, g);
   if (rc) return rc;
   const size_t zbytes = g.anchors * sizeof(T) + 64;
@@ -918,21 +958,24 @@ static int progressive_step_t(prism_prog* p, double target, const T* prev, T* va
   const double* range = reinterpret_cast<const double*>(tr + 8);
   bool first = p->steps == 0;
   StrategyState* ds = p->d_state;
+  // parameters alternate between two slots, so that the next step's plan can
+  // run while this step's reconstruction reads its own
+  PredParams<T>* params = reinterpret_cast<PredParams<T>*>((p->steps & 1) ? s->params_odd : s->params);
+  // ---- on the decode stream: strategy, plan, chunk offsets, decode, state
   if (first) {  // no planes loaded, all levels, no errors
-    prog_init_kernel<<<1, 32, 0, st>>>(ds, p->d_err);
+    prog_init_kernel<<<1, 32, 0, dst>>>(ds, p->d_err);
     h->launches += 1;
   }
   // strategy (findStrategy_h) from the container's cumulative plane sizes;
   // it advances the object's device state in place
   const uint64_t* csbp = reinterpret_cast<const uint64_t*>(tr + 16);
-  prof_begin(h, kStStrategy, st);
-  strategy_scan_kernel<<<dim3(kStrategyGroups, 33), 256, 0, st>>>(csbp, p->mode, p->bound, target, range, s->sblk);
+  prof_begin(h, kStStrategy, dst);
+  strategy_scan_kernel<<<dim3(kStrategyGroups, 33), 256, 0, dst>>>(csbp, p->mode, p->bound, target, range, s->sblk);
   // the strategy's plane ranges, then the parameters with its maxlevel
-  prog_plan_kernel<T><<<1, 32, 0, st>>>(s->sblk, p->mode, p->bound, target, range, ds,
-                                        alpha_of(p->mode == 1 ? p->bound : 0.0), tr,
-                                        reinterpret_cast<PredParams<T>*>(s->params), &s->eb,
-                                        p->exact ? s->dec_begin : nullptr);
-  prof_end(h, kStStrategy, st);
+  prog_plan_kernel<T><<<1, 32, 0, dst>>>(s->sblk, p->mode, p->bound, target, range, ds,
+                                         alpha_of(p->mode == 1 ? p->bound : 0.0), tr, params, &s->eb,
+                                         p->exact ? s->dec_begin : nullptr);
+  prof_end(h, kStStrategy, dst);
   h->launches += 2;
   // chunk offsets: once per object when it holds a slot
   const int64_t* offs = nullptr;
@@ -940,7 +983,7 @@ static int progressive_step_t(prism_prog* p, double target, const T* prev, T* va
     DevBuf& ob = h->prog_offs[p->slot];
     if (!p->offs_ready) {
       CKA(ob.ensure(((size_t)g.chunks + 1) * sizeof(int64_t)));
-      launch_chunk_offsets(h, p->cont, g, ob.as<int64_t>(), st);
+      launch_chunk_offsets(h, p->cont, g, ob.as<int64_t>(), dst);
       p->offs_ready = true;
     }
     offs = ob.as<int64_t>();
@@ -948,26 +991,33 @@ static int progressive_step_t(prism_prog* p, double target, const T* prev, T* va
   // chunks of planes the step does not load are written as zeros; the
   // inverse shuffle keeps planes [begin, end) of what was decoded
   rc = launch_decode(h, p->cont, p->size - g.header_size, g, p->exact ? s->dec_begin : ds->begin, ds->end,
-                     h->planes.as<uint8_t>(), st, p->d_err, offs);
+                     h->planes.as<uint8_t>(), dst, p->d_err, offs);
   if (rc) return rc;
+  // the state after the step (plane ranges, errors, bytes loaded) for the host
+  prog_publish_kernel<<<1, 32, 0, dst>>>(ds, p->d_err, csbp, p->mirror_dev);
+  h->launches += 1;
+  CK(cudaEventRecord(h->dec_done, dst));
+  // ---- on the caller's stream: inverse shuffle, reconstruction
+  CK(cudaStreamWaitEvent(st, h->dec_done, 0));
   rc = launch_inverse(h, h->planes.as<uint8_t>(), g, 1 /*NB*/, ds->begin, ds->end, h->qc.as<int32_t>(), st);
   if (rc) return rc;
+  CK(cudaEventRecord(h->planes_free, st));
   prof_begin(h, kStReconstruct, st);
   if (first) {
-    rc = launch_reconstruct<T, false>(h, h->qc.as<int32_t>(), reinterpret_cast<const T*>(tr + 1040), g,
-                                      params_ptr<T>(h), nullptr, values, st);
+    rc = launch_reconstruct<T, false>(h, h->qc.as<int32_t>(), reinterpret_cast<const T*>(tr + 1040), g, params,
+                                      nullptr, values, st);
   } else {
-    rc = launch_reconstruct<T, true>(h, h->qc.as<int32_t>(), h->zero_anchors.as<T>(), g, params_ptr<T>(h), prev,
-                                     values, st);
+    rc = launch_reconstruct<T, true>(h, h->qc.as<int32_t>(), h->zero_anchors.as<T>(), g, params, prev, values, st);
   }
   if (rc) return rc;
   prof_end(h, kStReconstruct, st);
-  prog_publish_kernel<<<1, 32, 0, st>>>(ds, p->d_err, csbp, p->mirror_dev);
-  h->launches += 1;
   CK(cudaGetLastError());
   CK(cudaEventRecord(p->done, st));
   p->pending = true;
   p->steps++;
+  h->chain_prog = p;
+  h->chain_stream = st;
+  h->chain_epoch = h->epoch;
   return PRISM_OK;
 }
 
