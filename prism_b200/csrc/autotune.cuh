@@ -198,7 +198,7 @@ __device__ __forceinline__ void compute_params(int mode, double bound, const dou
                                                const T* __restrict__ partial, int nwin,
                                                const uint8_t* __restrict__ flags_in, int maxlevel,
                                                PredParams<T>* __restrict__ out, T* __restrict__ errors_out,
-                                               double* __restrict__ eb_out) {
+                                               double* __restrict__ eb_out, const T* __restrict__ sums = nullptr) {
   using F = Fp<T>;
   PredParams<T> p;
   double eb = mode == 1 ? __dmul_rn(bound, *range) : bound;
@@ -219,11 +219,15 @@ __device__ __forceinline__ void compute_params(int mode, double bound, const dou
     p.ebr[level] = cr;
   }
   for (int l = 0; l < 4; ++l) p.natural[l] = 0;
-  if (partial) {
+  if (partial || sums) {
     T e[15];
     for (int k = 0; k < 15; ++k) {
       T s = T(0);
-      for (int w = 0; w < nwin; ++w) s = F::add(s, partial[(size_t)w * 15 + k]);
+      if (sums) {
+        s = sums[k];
+      } else {
+        for (int w = 0; w < nwin; ++w) s = F::add(s, partial[(size_t)w * 15 + k]);
+      }
       e[k] = s;
       if (errors_out) errors_out[k] = s;
     }
@@ -249,13 +253,26 @@ __device__ __forceinline__ void compute_params(int mode, double bound, const dou
   if (eb_out) *eb_out = eb;
 }
 
+// One warp: lane k < 15 sums variant k's errors over the windows in window
+// order (the same sums, in the same order, as a single thread would form),
+// then lane 0 decides.
 template <class T>
 __global__ void params_kernel(int mode, double bound, const double* __restrict__ range, double alpha,
                               const T* __restrict__ partial, int nwin, const uint8_t* __restrict__ flags_in,
                               int maxlevel, PredParams<T>* __restrict__ out, T* __restrict__ errors_out,
                               double* __restrict__ eb_out) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  compute_params<T>(mode, bound, range, alpha, partial, nwin, flags_in, maxlevel, out, errors_out, eb_out);
+  __shared__ T sums[15];
+  if (blockIdx.x != 0) return;
+  const int k = threadIdx.x;
+  if (partial && k < 15) {
+    T s = T(0);
+    for (int w = 0; w < nwin; ++w) s = Fp<T>::add(s, partial[(size_t)w * 15 + k]);
+    sums[k] = s;
+  }
+  __syncthreads();
+  if (k != 0) return;
+  compute_params<T>(mode, bound, range, alpha, partial, nwin, flags_in, maxlevel, out, errors_out, eb_out,
+                    partial ? sums : nullptr);
 }
 
 // Global min / max (compressor.cu:230-302): per-block partials, then one block.
