@@ -159,3 +159,26 @@ def test_exact_refinement_equals_one_step():
             assert d <= 16 * ulp and np.abs(two - data).max() <= 1e-4 * rng
         else:
             assert d > 1e-3 * rng and np.abs(two - data).max() > 1e-3 * rng
+
+
+@pytest.mark.parametrize("kind,shape,dtype,mode,bound", [
+    ("grf", (24, 40, 56), np.float64, 1, 1e-6),
+    ("sinusoid", (33, 40, 48), np.float32, 1, 1e-5),
+    ("voronoi", (30, 45, 50), np.float32, 0, 1e-4),
+    ("grf", (17, 33, 65), np.float32, 1, 1e-5),
+])
+def test_exact_chains_equal_one_step(kind, shape, dtype, mode, bound):
+    """Chains of three exact-refinement steps end every step within a few
+    ulps of the largest magnitude of the one-step retrieval to the same
+    planes, on shapes with and without 8-byte-multiple planes."""
+    from prism_b200 import fields
+    data = fields.make(kind, shape, dtype, 7)
+    cont, _, _ = O.compress(data, mode, bound, 0)
+    scale = 1.0 if mode == 1 else float(np.abs(data).max())
+    ulp = float(np.spacing(np.array(np.abs(data).max(), dtype=dtype)))
+    st = O.ProgressiveState()
+    for t in (1e-1, 1e-3, 1e-5):
+        got, (b, e, ml) = O.progressive_step(cont, shape, dtype, mode, bound, t * scale, st, exact=True)
+        one, (b1, e1, ml1) = O.progressive_step(cont, shape, dtype, mode, bound, t * scale, O.ProgressiveState())
+        assert e == e1
+        assert np.abs(got.astype(np.float64) - one).max() <= 16 * ulp, (t, np.abs(got.astype(np.float64) - one).max() / ulp)
