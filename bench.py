@@ -736,6 +736,7 @@ def run_serving(torch, P, args, nfields=32, rate=200.0, seconds=5.0, slots=4, po
             "service_p50_ms": st["service_p50_ms"], "service_p99_ms": st["service_p99_ms"],
             "requests_per_s": nreq / wall, "delivered_GBps": st["bytes_out"] / wall / 1e9,
             "cache_hits": st["cache_hits"], "shared": st["shared"], "refined": st["refined"],
+            "plane_search_calls": st["plan_calls"],
             "evictions": st["evictions"], "failed": st["failed"], "peak_resident_bytes": st["bytes_peak"],
             "container_bytes": int(sum(ctx_bytes for ctx_bytes in conts_bytes)),
             "data": "synthetic, generated on the device" + ("" if full else

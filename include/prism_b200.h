@@ -253,6 +253,15 @@ int prism_lossless_encode_static(const uint8_t* d_planes, uint32_t nx, uint32_t 
  * plane sizes (host), the absolute bound and the absolute target error. */
 int prism_find_strategy(prism_handle* h, const uint64_t comp_size_bp[128], double eb,
                         double target_error, int begin[4], int end[4], int* maxlevel, void* stream);
+/* Many strategy steps at once (no counterpart in the reference, which runs
+ * findStrategy_h, dataloader.cu:179-334, one target at a time): search i
+ * reads comp_size_bp[128 i .. 128 i + 127], the absolute bound eb[i] and
+ * target target_error[i], and updates begin[4 i ..], end[4 i ..] and
+ * maxlevel[i] (host arrays) exactly as prism_find_strategy would.  One scan
+ * launch and one reduction launch for all n (1 <= n <= 65535) searches, then
+ * a wait for `stream`. */
+int prism_find_strategy_batch(prism_handle* h, int n, const uint64_t* comp_size_bp, const double* eb,
+                              const double* target_error, int* begin, int* end, int* maxlevel, void* stream);
 
 /* Error statistics of a reconstruction against the original (both device
  * arrays of n values): out = {max |error|, max |error| / range, PSNR, NRMSE,
@@ -342,6 +351,8 @@ typedef struct prism_server_stats {
   double queue_p50_ms, queue_p99_ms;                  /* submit -> a slot takes it */
   double service_p50_ms, service_p99_ms;              /* slot start -> completion */
   uint64_t refined;                                   /* misses refined from a coarser entry */
+  uint64_t plan_calls;  /* batched plane searches run: each searches the plane selections of the request a
+                         * worker takes and of up to 31 other queued requests (prism_find_strategy_batch) */
 } prism_server_stats;
 
 /* hbm_budget: bytes of device memory the server may hold (containers,

@@ -74,6 +74,7 @@ def lib():
         l.prism_lossless_encode.argtypes = [vp, vp, u32, u32, u32, vp, u64, C.POINTER(u64), vp, vp]
         l.prism_lossless_decode.argtypes = [vp, vp, u32, u32, u32, vp, vp, vp, vp]
         l.prism_find_strategy.argtypes = [vp, vp, dbl, dbl, vp, vp, vp, vp]
+        l.prism_find_strategy_batch.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp, vp, vp]
         l.prism_lossless_encode_static.argtypes = [vp, u32, u32, u32, vp, u64, C.POINTER(u64), vp, vp]
         l.prism_lossless_wait_selftest.argtypes = [vp, vp, u32, u32, u32, vp, u64, C.c_longlong, vp]
         l.prism_extrema_minmax.argtypes = [vp, vp, i32, u64, vp, vp]
@@ -117,6 +118,7 @@ EXPORTED = [
     "prism_progressive_state", "prism_progressive_close", "prism_extrema", "prism_autotune",
     "prism_code_buffer_len", "prism_predict", "prism_reconstruct", "prism_bitshuffle",
     "prism_inverse_bitshuffle", "prism_lossless_encode", "prism_lossless_decode", "prism_find_strategy",
+    "prism_find_strategy_batch",
     "prism_profile", "prism_stage_times", "prism_launch_count", "prism_lossless_encode_static",
     "prism_batch_create", "prism_batch_compress", "prism_batch_schedule", "prism_batch_last_error",
     "prism_batch_destroy", "prism_server_create", "prism_server_add_field", "prism_server_submit",
@@ -448,7 +450,7 @@ class ServerStats(C.Structure):
                                           "bytes_resident", "bytes_reserved", "bytes_peak")] + \
                [(k, C.c_double) for k in ("p50_ms", "p99_ms", "mean_ms", "max_ms", "elapsed_s", "queue_p50_ms",
                                           "queue_p99_ms", "service_p50_ms", "service_p99_ms")] + \
-               [("refined", C.c_uint64)]
+               [("refined", C.c_uint64), ("plan_calls", C.c_uint64)]
 
 
 class Server:

@@ -93,6 +93,7 @@ struct ProgMirror {
 
 struct prism_handle {
   DevBuf qc, planes, status, offs, bsum, part, wins, ranges, anchors, small, dev_in, dev_out, zero_anchors;
+  DevBuf sbatch;  // batched strategy searches: cells, inputs and states
   // Pinned host memory mapped into the device: kernels store the results the
   // host reads (sizes, flags, parameters, progressive state) straight into
   // it, so reading them waits only for the kernels, never behind other
@@ -674,7 +675,8 @@ int prism_create(prism_handle** out) {
 void prism_destroy(prism_handle* h) {
   if (!h) return;
   DevBuf* bufs[] = {&h->qc, &h->planes, &h->status, &h->offs, &h->bsum, &h->part, &h->wins, &h->ranges,
-                    &h->anchors, &h->small, &h->dev_in, &h->dev_out, &h->zero_anchors, &h->prog_slots};
+                    &h->anchors, &h->small, &h->dev_in, &h->dev_out, &h->zero_anchors, &h->prog_slots,
+                    &h->sbatch};
   for (DevBuf* b : bufs) b->release();
   for (DevBuf& b : h->prog_offs) b.release();
   for (int i = 0; i < kStCount; ++i)
@@ -1390,6 +1392,61 @@ int prism_find_strategy(prism_handle* h, const uint64_t comp_size_bp[128], doubl
   return PRISM_OK;
 }
 
+
+int prism_find_strategy_batch(prism_handle* h, int n, const uint64_t* comp_size_bp, const double* eb,
+                              const double* target_error, int* begin, int* end, int* maxlevel, void* stream) {
+  if (!h || n < 1 || n > 65535 || !comp_size_bp || !eb || !target_error || !begin || !end || !maxlevel)
+    return PRISM_ERR_ARG;
+  for (int i = 0; i < n; ++i)
+    if (!(eb[i] > 0)) return PRISM_ERR_ARG;
+  ++h->epoch;
+  cudaStream_t st = (cudaStream_t)stream;
+  // device layout: cells | plane sizes | bound, target pairs | states | 1.0
+  const size_t cells = (size_t)n * kStrategyCells * sizeof(StrategyBest);
+  const size_t in_bytes = (size_t)n * 128 * sizeof(uint64_t) + (size_t)n * 2 * sizeof(double) +
+                          (size_t)n * sizeof(StrategyState) + sizeof(double);
+  CKA(h->sbatch.ensure(cells + in_bytes + 64));
+  std::vector<uint8_t> host(in_bytes);
+  uint8_t* q = host.data();
+  memcpy(q, comp_size_bp, (size_t)n * 128 * sizeof(uint64_t));
+  double* bt = reinterpret_cast<double*>(q + (size_t)n * 128 * sizeof(uint64_t));
+  for (int i = 0; i < n; ++i) {
+    bt[2 * i] = eb[i];
+    bt[2 * i + 1] = target_error[i];
+  }
+  StrategyState* ss = reinterpret_cast<StrategyState*>(bt + 2 * (size_t)n);
+  for (int i = 0; i < n; ++i) {
+    for (int l = 0; l < 4; ++l) {
+      ss[i].begin[l] = begin[4 * i + l];
+      ss[i].end[l] = end[4 * i + l];
+    }
+    ss[i].maxlevel = maxlevel[i];
+  }
+  double* one = reinterpret_cast<double*>(ss + n);
+  *one = 1.0;
+  uint8_t* d = h->sbatch.as<uint8_t>();
+  StrategyBest* d_cells = reinterpret_cast<StrategyBest*>(d);
+  uint8_t* d_in = d + cells;
+  const uint64_t* d_cs = reinterpret_cast<const uint64_t*>(d_in);
+  const double* d_bt = reinterpret_cast<const double*>(d_in + (size_t)n * 128 * sizeof(uint64_t));
+  StrategyState* d_ss = reinterpret_cast<StrategyState*>(const_cast<double*>(d_bt) + 2 * (size_t)n);
+  const double* d_one = reinterpret_cast<const double*>(d_ss + n);
+  CK(cudaMemcpyAsync(d_in, host.data(), in_bytes, cudaMemcpyHostToDevice, st));
+  strategy_scan_batch_kernel<<<dim3(kStrategyGroups, 33, n), 256, 0, st>>>(d_cs, d_bt, d_one, d_cells);
+  strategy_finish_batch_kernel<<<n, 32, 0, st>>>(d_cells, d_bt, d_one, d_ss);
+  h->launches += 2;
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(ss, d_ss, (size_t)n * sizeof(StrategyState), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  for (int i = 0; i < n; ++i) {
+    for (int l = 0; l < 4; ++l) {
+      begin[4 * i + l] = ss[i].begin[l];
+      end[4 * i + l] = ss[i].end[l];
+    }
+    maxlevel[i] = ss[i].maxlevel;
+  }
+  return PRISM_OK;
+}
 
 // ---------------------------------------------------------------------------
 // Lossless encode without any allocation (prism_lossless_encode_static).

@@ -73,7 +73,16 @@ struct SrvRequest {
   SrvClock::time_point t_submit, t_start, t_done;
   int end[4] = {0, 0, 0, 0};
   int maxlevel = 0;
+  // plane selection: 0 not searched, 1 being searched (in another worker's
+  // batch), 2 done (plan_* hold the result)
+  int plan = 0;
+  int plan_rc = 0;
+  int plan_end[4] = {0, 0, 0, 0};
+  int plan_maxlevel = 4;
 };
+
+// requests whose plane selections one worker searches in one batch
+constexpr int kPlanBatch = 32;
 
 // Handle workspace one slot needs for a field (what prism_progressive_step
 // allocates: codes, planes, chunk tables, anchors, small state).
@@ -107,6 +116,7 @@ struct prism_server {
   // statistics
   std::vector<double> lat_ms, queue_ms, service_ms;
   uint64_t completed = 0, hits = 0, shared = 0, evictions = 0, failed = 0, bytes_out = 0, refined = 0;
+  uint64_t plan_calls = 0;  // batched plane searches run (each for up to kPlanBatch requests)
   SrvClock::time_point t0;
   std::string err;
 };
@@ -144,14 +154,53 @@ void srv_worker(prism_server* s, int slot) {
     s->queue.pop_front();
     r->t_start = SrvClock::now();
     const SrvField f = s->fields[r->field];  // a copy: add_field may grow the vector
+    // Plane selection of the one-step retrieval (the strategy of
+    // prism_progressive_step from no planes, in absolute terms).  A request
+    // not yet searched is searched together with up to kPlanBatch - 1 other
+    // queued requests in one prism_find_strategy_batch call; a request that
+    // another worker's batch is searching is waited for.
+    std::vector<SrvRequest*> batch;
+    std::vector<uint64_t> b_cs;
+    std::vector<double> b_eb, b_te;
+    if (r->plan == 0) {
+      auto add = [&](SrvRequest* q) {
+        const SrvField& fq = s->fields[q->field];
+        q->plan = 1;
+        batch.push_back(q);
+        b_cs.insert(b_cs.end(), fq.csbp, fq.csbp + 128);
+        b_eb.push_back(fq.mode == 1 ? fq.bound * fq.range : fq.bound);
+        b_te.push_back(fq.mode == 1 ? q->target * fq.range : q->target);
+      };
+      add(r);
+      for (SrvRequest* q : s->queue) {
+        if ((int)batch.size() >= kPlanBatch) break;
+        if (q->plan == 0) add(q);
+      }
+    } else {
+      s->cv_done.wait(lk, [&] { return r->plan == 2; });
+    }
     lk.unlock();
     std::unique_lock<std::mutex> slot_lk(*s->slot_mu[slot]);
-    // plane selection of the one-step retrieval (the strategy of
-    // prism_progressive_step from no planes, in absolute terms)
-    int begin[4] = {0, 0, 0, 0}, end[4] = {0, 0, 0, 0}, maxlevel = 4;
-    const double eb = f.mode == 1 ? f.bound * f.range : f.bound;
-    const double te = f.mode == 1 ? r->target * f.range : r->target;
-    int rc = prism_find_strategy(h, f.csbp, eb, te, begin, end, &maxlevel, st);
+    if (!batch.empty()) {
+      const int nb = (int)batch.size();
+      std::vector<int> bb(4 * nb, 0), be(4 * nb, 0), bm(nb, 4);
+      const int brc = prism_find_strategy_batch(h, nb, b_cs.data(), b_eb.data(), b_te.data(), bb.data(), be.data(),
+                                                bm.data(), st);
+      lk.lock();
+      ++s->plan_calls;
+      for (int i = 0; i < nb; ++i) {
+        SrvRequest* q = batch[i];
+        q->plan_rc = brc;
+        std::copy(be.begin() + 4 * i, be.begin() + 4 * i + 4, q->plan_end);
+        q->plan_maxlevel = bm[i];
+        q->plan = 2;
+      }
+      s->cv_done.notify_all();
+      lk.unlock();
+    }
+    int end[4], maxlevel = r->plan_maxlevel;
+    std::copy(r->plan_end, r->plan_end + 4, end);
+    int rc = r->plan_rc;
     lk.lock();
     SrvEntry* e = nullptr;
     if (!rc) {
@@ -452,6 +501,7 @@ int prism_server_stats_get(prism_server* s, prism_server_stats* out, int reset) 
   out->bytes_peak = s->peak;
   out->elapsed_s = std::chrono::duration<double>(SrvClock::now() - s->t0).count();
   out->refined = s->refined;
+  out->plan_calls = s->plan_calls;
   auto pct = [](std::vector<double> v, double p) {
     if (v.empty()) return 0.0;
     std::sort(v.begin(), v.end());
@@ -473,7 +523,7 @@ int prism_server_stats_get(prism_server* s, prism_server_stats* out, int reset) 
     s->lat_ms.clear();
     s->queue_ms.clear();
     s->service_ms.clear();
-    s->completed = s->hits = s->shared = s->evictions = s->failed = s->bytes_out = s->refined = 0;
+    s->completed = s->hits = s->shared = s->evictions = s->failed = s->bytes_out = s->refined = s->plan_calls = 0;
     s->t0 = SrvClock::now();
   }
   return PRISM_OK;

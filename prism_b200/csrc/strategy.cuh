@@ -77,9 +77,10 @@ __device__ __forceinline__ bool strategy_better(unsigned long long v, unsigned k
   return v > bv || (v == bv && k > bk);
 }
 
-__global__ void __launch_bounds__(256)
-strategy_scan_kernel(const uint64_t* __restrict__ cs, int mode, double bound, double target,
-                     const double* __restrict__ range, StrategyBest* __restrict__ out) {
+// One CTA of the scan: group of rounds `group`, first-level plane count b0.
+__device__ __forceinline__ void strategy_scan_cta(const uint64_t* __restrict__ cs, int mode, double bound,
+                                                  double target, const double* __restrict__ range,
+                                                  StrategyBest* __restrict__ out, const int group, const int b0) {
   bool use_search;
   uint64_t target_cost;
   strategy_setup(mode, bound, target, range, &use_search, &target_cost);
@@ -88,7 +89,7 @@ strategy_scan_kernel(const uint64_t* __restrict__ cs, int mode, double bound, do
   __shared__ uint64_t vt[4][33];
   __shared__ unsigned long long wv[8];
   __shared__ unsigned wk[8];
-  const int tid = threadIdx.x, group = blockIdx.x, b0 = blockIdx.y;
+  const int tid = threadIdx.x;
   if (tid < 4 * 33) {
     int l = tid / 33, b = tid % 33;
     cost[l][b] = strategy_cost(l, b);
@@ -134,6 +135,23 @@ strategy_scan_kernel(const uint64_t* __restrict__ cs, int mode, double bound, do
     r.pad = 0;
     out[b0 * kStrategyGroups + group] = r;
   }
+}
+
+__global__ void __launch_bounds__(256)
+strategy_scan_kernel(const uint64_t* __restrict__ cs, int mode, double bound, double target,
+                     const double* __restrict__ range, StrategyBest* __restrict__ out) {
+  strategy_scan_cta(cs, mode, bound, target, range, out, blockIdx.x, blockIdx.y);
+}
+
+// Many independent searches in one launch (grid z = search): search i reads
+// cumulative plane sizes cs + 128 i and the absolute bound / target
+// bt[2 i], bt[2 i + 1], and writes its cells to out + kStrategyCells i.
+__global__ void __launch_bounds__(256)
+strategy_scan_batch_kernel(const uint64_t* __restrict__ cs, const double* __restrict__ bt,
+                           const double* __restrict__ one, StrategyBest* __restrict__ out) {
+  const int i = blockIdx.z;
+  strategy_scan_cta(cs + 128 * (size_t)i, 0, bt[2 * i], bt[2 * i + 1], one, out + (size_t)kStrategyCells * i,
+                    blockIdx.x, blockIdx.y);
 }
 
 // Reduction over the cells + begin/end/maxlevel update
@@ -198,6 +216,13 @@ __global__ void strategy_finish_kernel(const StrategyBest* __restrict__ cells, i
                                        double target, const double* __restrict__ range,
                                        StrategyState* __restrict__ st) {
   strategy_finish_warp(cells, mode, bound, target, range, st);
+}
+
+// one warp per search of strategy_scan_batch_kernel
+__global__ void strategy_finish_batch_kernel(const StrategyBest* __restrict__ cells, const double* __restrict__ bt,
+                                             const double* __restrict__ one, StrategyState* __restrict__ st) {
+  const int i = blockIdx.x;
+  strategy_finish_warp(cells + (size_t)kStrategyCells * i, 0, bt[2 * i], bt[2 * i + 1], one, st + i);
 }
 
 }  // namespace prism_b200

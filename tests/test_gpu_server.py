@@ -100,6 +100,8 @@ def run_mix(torch, P, flds, reqs, refine, first=()):
     st = srv.stats()
     srv.close()
     assert st["completed"] == len(first) + len(reqs) and st["failed"] == 0
+    # plane selections are searched in batches of queued requests
+    assert 1 <= st["plan_calls"] <= st["completed"]
     assert st["bytes_peak"] <= budget
     assert 0 < st["p50_ms"] <= st["p99_ms"]
     return outs, infos, st

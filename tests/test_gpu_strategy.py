@@ -78,3 +78,47 @@ def test_strategy_matches_oracle_in_sequence(env):
             gb, ge, gml = gpu_strategy(torch, P, h, cs, eb, r * eb, gb, ge)
             ob, oe, oml = O.find_strategy(cs, eb, r * eb, ob, oe)
             assert (gb, ge, gml) == (ob, oe, oml), (r, gb, ge, gml, ob, oe, oml)
+
+
+def test_batched_strategy_matches_oracle(env):
+    """prism_find_strategy_batch: every (table, ratio) search of the single-step
+    test plus searches from mid-sequence states, all in one call, each equal to
+    the oracle's step."""
+    torch, P, h = env
+    eb = 1e-6
+    cases = []
+    for cs in tables():
+        for r in RATIOS:
+            cases.append((cs, eb, r * eb, [0] * 4, [0] * 4))
+        b, e = [0] * 4, [0] * 4
+        for r in [1e7, 1e5, 3e3]:
+            b, e, _ = O.find_strategy(cs, eb, r * eb, b, e)
+        for r in [40.0, 1.0]:
+            cases.append((cs, eb, r * eb, list(b), list(e)))
+    n = len(cases)
+    cs_all = np.ascontiguousarray(np.stack([c[0] for c in cases]), dtype=np.uint64)
+    ebs = np.array([c[1] for c in cases], dtype=np.float64)
+    tgs = np.array([c[2] for c in cases], dtype=np.float64)
+    begin = np.array([c[3] for c in cases], dtype=np.int32).reshape(-1)
+    end = np.array([c[4] for c in cases], dtype=np.int32).reshape(-1)
+    ml = np.full(n, 4, dtype=np.int32)
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    vp = lambda a: a.ctypes.data_as(C.c_void_p)
+    h.check(P.lib().prism_find_strategy_batch(h.ptr, n, vp(cs_all), vp(ebs), vp(tgs), vp(begin), vp(end), vp(ml),
+                                              st), "prism_find_strategy_batch")
+    for i, (cs, e_b, tg, b0, e0) in enumerate(cases):
+        want = O.find_strategy(cs, e_b, tg, b0, e0)
+        got = (list(begin[4 * i: 4 * i + 4]), list(end[4 * i: 4 * i + 4]), int(ml[i]))
+        assert got == (list(want[0]), list(want[1]), want[2]), (i, got, want)
+
+
+def test_batched_strategy_rejects_bad_arguments(env):
+    torch, P, h = env
+    z = np.zeros(128, dtype=np.uint64)
+    one = np.ones(1)
+    b = np.zeros(4, dtype=np.int32)
+    ml = np.zeros(1, dtype=np.int32)
+    vp = lambda a: a.ctypes.data_as(C.c_void_p)
+    assert P.lib().prism_find_strategy_batch(h.ptr, 0, vp(z), vp(one), vp(one), vp(b), vp(b), vp(ml), None) != 0
+    assert P.lib().prism_find_strategy_batch(h.ptr, 1, vp(z), vp(np.zeros(1)), vp(one), vp(b), vp(b), vp(ml),
+                                             None) != 0
