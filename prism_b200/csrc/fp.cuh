@@ -20,6 +20,8 @@ template <> struct Fp<float> {
   static __device__ __forceinline__ int to_int_rz(float a) { return __float2int_rz(a); }
   static __device__ __forceinline__ float from_int(int a) { return __int2float_rn(a); }
   static __device__ __forceinline__ float from_double(double a) { return __double2float_rn(a); }
+  // a value whose bits are the 32-bit word w (a code parked in a value slot)
+  static __device__ __forceinline__ float with_low_word(int w) { return __int_as_float(w); }
 };
 
 template <> struct Fp<double> {
@@ -32,6 +34,8 @@ template <> struct Fp<double> {
   static __device__ __forceinline__ int to_int_rz(double a) { return __double2int_rz(a); }
   static __device__ __forceinline__ double from_int(int a) { return __int2double_rn(a); }
   static __device__ __forceinline__ double from_double(double a) { return a; }
+  // a value whose low word is w and whose high word is zero
+  static __device__ __forceinline__ double with_low_word(int w) { return __hiloint2double(0, w); }
 };
 
 }  // namespace prism_b200

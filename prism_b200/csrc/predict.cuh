@@ -1371,9 +1371,50 @@ reconstruct_kernel(const int32_t* __restrict__ qc, const T* __restrict__ anchors
   copy_async_commit();
   // Level-0 codes by window rows r = z*17 + y: a row with y or z odd holds
   // 17 level-0 points at consecutive slots rows[r] + x, a row with both even
-  // its 8 odd-x points at rows[r] + x/2.  Each half-warp takes x = 0..15 of
-  // one row (the row's slot base is one shared broadcast), then x = 16.
-  {
+  // its 8 odd-x points at rows[r] + x/2.
+  if (sizeof(T) == 4 && !EDGE && maxlevel >= 0 && (reinterpret_cast<uintptr_t>(qc) & 15) == 0) {
+    // Float interior tile, 16-byte aligned codes: a row's codes lie in at
+    // most five aligned 16-byte chunks (offset o = rows[r] mod 4 plus 17
+    // codes), and chunk s of the tile is chunk s mod 5 of row s / 5.  A
+    // thread's loads are in flight three at a time before their stores; the
+    // words a chunk holds beyond the row (neighbouring rows' codes, or the
+    // code buffer's slack past the last slot) are not stored.  A third of the
+    // fetch instructions of the copies below, but the codes must arrive
+    // before the coarse levels start: faster for float tiles (seven per SM),
+    // slower for double ones (five per SM hide less of that wait).
+    constexpr int kChunks = kWin * kWin * 5, kIt = (kChunks + kPredThreads - 1) / kPredThreads;
+    constexpr int kBatch = (kIt + 1) / 2;
+#pragma unroll
+    for (int k0 = 0; k0 < kIt; k0 += kBatch) {
+      int4 v[kBatch];
+#pragma unroll
+      for (int k = 0; k < kBatch; ++k) {
+        const int s = tid + (k0 + k) * kPredThreads, r = s / 5, c = s - 5 * r;
+        v[k] = make_int4(0, 0, 0, 0);
+        if (k0 + k < kIt && s < kChunks) {
+          const int y = r % kWin, z = r / kWin, n = ((y | z) & 1) ? kWin : 8;
+          const uint64_t first = sm.rows[r];
+          const int o = (int)(first & 3);
+          if (4 * c < o + n) v[k] = __ldg(reinterpret_cast<const int4*>(qc + (first - o)) + c);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < kBatch; ++k) {
+        const int s = tid + (k0 + k) * kPredThreads, r = s / 5, c = s - 5 * r;
+        if (k0 + k >= kIt || s >= kChunks) continue;
+        const int y = r % kWin, z = r / kWin, ee = ((y | z) & 1) == 0, n = ee ? 8 : kWin;
+        const int o = (int)(sm.rows[r] & 3);
+        const int32_t w[4] = {v[k].x, v[k].y, v[k].z, v[k].w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const int xi = 4 * c + i - o;
+          if (xi >= 0 && xi < n) sm.win[Win<T>::at(ee ? 2 * xi + 1 : xi, y, z)] = Fp<T>::with_low_word(w[i]);
+        }
+      }
+    }
+  } else {
+    // Each half-warp takes x = 0..15 of one row (the row's slot base is one
+    // shared broadcast), then x = 16.
     static_assert(2 * (kPredThreads / 32) == 16, "rows advance by 16: (y, z) -> (y - 1, z + 1) or (16, z)");
     const int lane = tid & 31, x = lane & 15;
     const bool codes = maxlevel >= 0;
@@ -1449,24 +1490,26 @@ reconstruct_kernel(const int32_t* __restrict__ qc, const T* __restrict__ anchors
       return;
     }
   }
+  // The tile's points (16 per axis, plus the plane at 16 on the field's last
+  // slab along that axis), enumerated over a fixed box so the coordinates
+  // come from constant divisors.
+  constexpr int kB = EDGE ? kWin : 16, kBox = kB * kB * kB;
   const int xs = 16 + (EDGE && f.last[0]), ys = 16 + (EDGE && f.last[1]), zs = 16 + (EDGE && f.last[2]);
-  const int total = xs * ys * zs;
-  for (int b = tid; b < total; b += kPrefetch * kPredThreads) {
+  for (int b = tid; b < kBox; b += kPrefetch * kPredThreads) {
     T o[kPrefetch];
     if (PROG) {
 #pragma unroll
       for (int k = 0; k < kPrefetch; ++k) {
-        int i = b + k * kPredThreads;
-        int x = i % xs, y = (i / xs) % ys, z = i / (xs * ys);
+        const int i = b + k * kPredThreads, x = i % kB, y = (i / kB) % kB, z = i / (kB * kB);
         o[k] = T(0);
-        if (i < total && L.in_data(x, y, z)) o[k] = old[base + x + (uint64_t)y * sy + (uint64_t)z * sz];
+        if (i < kBox && x < xs && y < ys && z < zs && L.in_data(x, y, z))
+          o[k] = old[base + x + (uint64_t)y * sy + (uint64_t)z * sz];
       }
     }
 #pragma unroll
     for (int k = 0; k < kPrefetch; ++k) {
-      int i = b + k * kPredThreads;
-      int x = i % xs, y = (i / xs) % ys, z = i / (xs * ys);
-      if (i >= total || !L.in_data(x, y, z)) continue;
+      const int i = b + k * kPredThreads, x = i % kB, y = (i / kB) % kB, z = i / (kB * kB);
+      if (i >= kBox || x >= xs || y >= ys || z >= zs || !L.in_data(x, y, z)) continue;
       T v = sm.win[Win<T>::at(x, y, z)];
       out[base + x + (uint64_t)y * sy + (uint64_t)z * sz] = PROG ? Fp<T>::add(v, o[k]) : v;
     }
