@@ -217,9 +217,14 @@ __device__ __noinline__ void batch_tile_call(CompressSmem<T>& sm, Geometry& sg, 
 }
 
 // Predictor over the tiles of part PART (0 interior, 1 edge) of every group
-// field, one CTA per tile.
+// field, one CTA per tile.  Float edge tiles keep four CTAs per SM here (56
+// registers, no spills): with the field lookup, six would spill 172 bytes a
+// thread, a variant not measured in this kernel.
 template <class T, int PART>
-__global__ void __launch_bounds__(kPredThreads, predict_min_ctas<T, PART>())
+constexpr int batch_predict_min_ctas() { return sizeof(T) == 4 && PART == 0 ? 6 : 4; }
+
+template <class T, int PART>
+__global__ void __launch_bounds__(kPredThreads, batch_predict_min_ctas<T, PART>())
 batch_predict_kernel(const BatchField* __restrict__ fields, const int* __restrict__ gidx,
                      const uint64_t* __restrict__ prefix, int n, uint64_t items) {
   extern __shared__ __align__(16) unsigned char smem_raw[];

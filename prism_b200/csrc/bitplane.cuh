@@ -72,6 +72,31 @@ __device__ __forceinline__ void bit_transpose32(uint32_t (&a)[32]) {
 // order, most significant bit first).
 __device__ __forceinline__ constexpr int plane_bit_code(int k) { return 8 * (k >> 3) + 7 - (k & 7); }
 
+// 8x8 bit transposes of the four byte columns of eight words at once (delta
+// swaps of 4-, 2- and 1-bit blocks between rows i and i + s): afterwards
+// byte c of w[j] bit i = (before) w[i] bit 8c + j.
+__device__ __forceinline__ void bit_transpose8x4(uint32_t (&w)[8]) {
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const uint32_t t = ((w[i] >> 4) ^ w[i + 4]) & 0x0F0F0F0Fu;
+    w[i + 4] ^= t;
+    w[i] ^= t << 4;
+  }
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    if (i & 2) continue;
+    const uint32_t t = ((w[i] >> 2) ^ w[i + 2]) & 0x33333333u;
+    w[i + 2] ^= t;
+    w[i] ^= t << 2;
+  }
+#pragma unroll
+  for (int i = 0; i < 8; i += 2) {
+    const uint32_t t = ((w[i] >> 1) ^ w[i + 1]) & 0x55555555u;
+    w[i + 1] ^= t;
+    w[i] ^= t << 1;
+  }
+}
+
 
 // a[i] of a 4-entry array held in kernel parameters, without the local-memory
 // copy a dynamic index would force
@@ -186,7 +211,7 @@ bitshuffle_kernel(const int32_t* __restrict__ codes, uint8_t* __restrict__ plane
 __global__ void __launch_bounds__(kShufWarps * 32, 4)
 inverse_bitshuffle_kernel(const uint8_t* __restrict__ planes, int32_t* __restrict__ codes, Geometry g,
                           ShufPlan plan, int nb, const int* __restrict__ begin, const int* __restrict__ end) {
-  __shared__ uint32_t tile[kShufWarps][32][33];
+  __shared__ __align__(16) uint32_t tile[kShufWarps][32][33];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int64_t item = (int64_t)blockIdx.x * kShufWarps + warp;
   if (item >= plan.items) return;
@@ -207,33 +232,75 @@ inverse_bitshuffle_kernel(const uint8_t* __restrict__ planes, int32_t* __restric
   const int64_t stride = pick4(g.dstride, level);
   const uint8_t* base = planes + pick4(g.daprefix, level) + first / 8;
   uint32_t (&tw)[32][33] = tile[warp];
-  // a[r] = the lane's word (as loaded) of plane 31 - r
+  const bool full = count == kShufCodes;
+  // a[k] = transformed code 32 lane + plane_bit_code(k) (code bit b from
+  // plane 31 - b, bit k of the lane's word)
   uint32_t a[32];
-  if (count == kShufCodes) {  // every item but a level's last: one word per lane and plane
+  if (full && hi - lo <= 8) {
+    // At most eight planes (a refinement step): they lie in the eight code
+    // bits r0..r0+7, w[i] = the lane's word of plane 31 - r0 - i, and one
+    // 8x8 transpose per byte column gives every code's byte.
+    const int r0 = min(32 - hi, 24);
+    uint32_t w[8];
 #pragma unroll
-    for (int r = 0; r < 32; ++r) {
-      const int p = 31 - r;
-      a[r] = (p >= lo && p < hi) ? __ldg(reinterpret_cast<const uint32_t*>(base + (int64_t)p * stride) + lane) : 0u;
+    for (int i = 0; i < 8; ++i) {
+      const int p = 31 - r0 - i;
+      w[i] = (p >= lo && p < hi) ? __ldg(reinterpret_cast<const uint32_t*>(base + (int64_t)p * stride) + lane) : 0u;
     }
+    bit_transpose8x4(w);
+#pragma unroll
+    for (int k = 0; k < 32; ++k) a[k] = __byte_perm(w[k & 7], 0u, 0x4440 | (k >> 3)) << r0;
   } else {
+    // a[r] = the lane's word (as loaded) of plane 31 - r
+    if (full) {  // every item but a level's last: one word per lane and plane
 #pragma unroll
-    for (int r = 0; r < 32; ++r) {
-      const int p = 31 - r;
-      const uint8_t* src = base + (int64_t)p * stride;
-      uint32_t v = 0;
-      if (p >= lo && p < hi) {
-        if (4 * lane + 4 <= nbytes) {
-          v = __ldg(reinterpret_cast<const uint32_t*>(src) + lane);
-        } else if (4 * lane < nbytes) {
-          for (int b = 4 * lane; b < nbytes; ++b) v |= (uint32_t)src[b] << (8 * (b & 3));
-        }
+      for (int r = 0; r < 32; ++r) {
+        const int p = 31 - r;
+        a[r] = (p >= lo && p < hi) ? __ldg(reinterpret_cast<const uint32_t*>(base + (int64_t)p * stride) + lane) : 0u;
       }
-      a[r] = v;
+    } else {
+#pragma unroll
+      for (int r = 0; r < 32; ++r) {
+        const int p = 31 - r;
+        const uint8_t* src = base + (int64_t)p * stride;
+        uint32_t v = 0;
+        if (p >= lo && p < hi) {
+          if (4 * lane + 4 <= nbytes) {
+            v = __ldg(reinterpret_cast<const uint32_t*>(src) + lane);
+          } else if (4 * lane < nbytes) {
+            for (int b = 4 * lane; b < nbytes; ++b) v |= (uint32_t)src[b] << (8 * (b & 3));
+          }
+        }
+        a[r] = v;
+      }
     }
+    bit_transpose32(a);
   }
-  bit_transpose32(a);
-  // a[k] = transformed code 32 lane + plane_bit_code(k); out through the tile
-  // so that the codes leave in coalesced rows
+  if (full && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+    // Out through the tile in 16-byte pieces: row l holds lane l's codes
+    // 32l..32l+31, its four-code block q at block q ^ (l mod 8) (each
+    // quarter-warp touches eight distinct bank groups on both sides), and
+    // each warp store writes 512 consecutive bytes.
+    uint32_t* tv = &tw[0][0];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      uint4 v;
+      v.x = (uint32_t)sign_inverse(a[plane_bit_code(4 * q)], nb);
+      v.y = (uint32_t)sign_inverse(a[plane_bit_code(4 * q + 1)], nb);
+      v.z = (uint32_t)sign_inverse(a[plane_bit_code(4 * q + 2)], nb);
+      v.w = (uint32_t)sign_inverse(a[plane_bit_code(4 * q + 3)], nb);
+      *reinterpret_cast<uint4*>(tv + 32 * lane + 4 * (q ^ (lane & 7))) = v;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int s = 0; s < 8; ++s) {
+      const int row = 4 * s + (lane >> 3);
+      reinterpret_cast<uint4*>(dst)[32 * s + lane] =
+          *reinterpret_cast<const uint4*>(tv + 32 * row + 4 * ((lane & 7) ^ (row & 7)));
+    }
+    return;
+  }
+  // out through the padded tile, so that the codes leave in coalesced rows
 #pragma unroll
   for (int k = 0; k < 32; ++k) tw[lane][plane_bit_code(k)] = a[k];
   __syncwarp();

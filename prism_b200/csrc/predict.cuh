@@ -1299,12 +1299,12 @@ __device__ __forceinline__ void compress_tile(CompressSmem<T>& sm, const T* __re
   }
 }
 
-// CTAs per SM the compiler must leave room for: a float interior tile's
-// shared memory (window + codes, 36 KB) admits six on an SM when its registers
-// do; double tiles (55 KB) and edge tiles are held to fewer by shared memory
-// and their runtime limits.
+// CTAs per SM the compiler must leave room for: a float tile's shared memory
+// (window + codes, 36 KB) admits six on an SM when its registers do, a double
+// one (55 KB) four.  For float last-slab tiles six (40 registers, a few
+// spilled) measured 7-9% faster than four (55 registers).
 template <class T, int PART>
-constexpr int predict_min_ctas() { return sizeof(T) == 4 && PART == 0 ? 6 : 4; }
+constexpr int predict_min_ctas() { return sizeof(T) == 4 ? 6 : 4; }
 
 template <class T, int PART>
 __global__ void __launch_bounds__(kPredThreads, predict_min_ctas<T, PART>())
@@ -1322,9 +1322,11 @@ predict_compress_kernel(const T* __restrict__ data, Geometry g, const PredParams
 // :2209-2239, shmem2global_data_progressive :1123-1147).  All codes the tile
 // can use are fetched up front with asynchronous copies.
 // a float interior tile's 23 KB of shared memory leaves room for seven
-// CTAs on an SM when its registers do; a double one (43 KB) for five
+// CTAs on an SM when its registers do; a double one (43 KB) for five.  The
+// last-slab tiles, with more live state, take six (float) and five (double):
+// 2-3% faster than four at 64 registers, with a few registers spilled.
 template <class T, int PART>
-constexpr int reconstruct_min_ctas() { return PART == 0 ? (sizeof(T) == 4 ? 7 : 5) : 4; }
+constexpr int reconstruct_min_ctas() { return PART == 0 ? (sizeof(T) == 4 ? 7 : 5) : (sizeof(T) == 4 ? 6 : 5); }
 
 
 template <class T, bool PROG, int PART>
