@@ -1291,11 +1291,22 @@ __device__ __forceinline__ void compress_tile(CompressSmem<T>& sm, const T* __re
   uint64_t* rows = reinterpret_cast<uint64_t*>(sm.win);
   fill_rows(g, f, rows);
   __syncthreads();
+  // Thread t takes point (t mod 16, t / 16) of each z-plane: a row with y or z
+  // odd is all level 0 (slot rows[r] + x), the odd x of the other rows too
+  // (rows[r] + x / 2); only the even x of those go through the level lookup.
   for (int i = tid; i < 16 * 16 * 16; i += kPredThreads) {
     const int x = i & 15, y = (i >> 4) & 15, z = i >> 8;
-    const int lv = win_level(x, y, z);
-    if (lv == 4 || !L.in_data(x, y, z)) continue;
-    qc[slot_of(rows, lv, x, y, z)] = sm.cw[cw_word(i)];
+    if (!L.in_data(x, y, z)) continue;
+    uint64_t slot;
+    if (((x | y | z) & 1) != 0) {
+      const int ee = ((y | z) & 1) == 0;
+      slot = rows[z * kWin + y] + (uint64_t)(x >> ee);
+    } else {
+      const int lv = win_level(x, y, z);
+      if (lv == 4) continue;
+      slot = slot_of(rows, lv, x, y, z);
+    }
+    qc[slot] = sm.cw[cw_word(i)];
   }
 }
 
@@ -1329,6 +1340,47 @@ template <class T, int PART>
 constexpr int reconstruct_min_ctas() { return PART == 0 ? (sizeof(T) == 4 ? 7 : 5) : (sizeof(T) == 4 ? 6 : 5); }
 
 
+// The level-0 codes of an interior tile from a 16-byte aligned code buffer:
+// a row's codes lie in at most five aligned 16-byte chunks (offset o =
+// rows[r] mod 4 plus 17 codes, or 8 on a row with y and z even), and chunk s
+// of the tile is chunk s mod 5 of row s / 5.  A thread's loads are in flight
+// three at a time before their stores; the words a chunk holds beyond the
+// row (neighbouring rows' codes, or the code buffer's slack past the last
+// slot) are not stored.
+template <class T>
+__device__ __forceinline__ void fetch_level0_vec(ReconSmem<T>& sm, const int32_t* __restrict__ qc, int tid) {
+  constexpr int kChunks = kWin * kWin * 5, kIt = (kChunks + kPredThreads - 1) / kPredThreads;
+  constexpr int kBatch = (kIt + 1) / 2;
+#pragma unroll
+  for (int k0 = 0; k0 < kIt; k0 += kBatch) {
+    int4 v[kBatch];
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k) {
+      const int s = tid + (k0 + k) * kPredThreads, r = s / 5, c = s - 5 * r;
+      v[k] = make_int4(0, 0, 0, 0);
+      if (k0 + k < kIt && s < kChunks) {
+        const int y = r % kWin, z = r / kWin, n = ((y | z) & 1) ? kWin : 8;
+        const uint64_t first = sm.rows[r];
+        const int o = (int)(first & 3);
+        if (4 * c < o + n) v[k] = __ldg(reinterpret_cast<const int4*>(qc + (first - o)) + c);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kBatch; ++k) {
+      const int s = tid + (k0 + k) * kPredThreads, r = s / 5, c = s - 5 * r;
+      if (k0 + k >= kIt || s >= kChunks) continue;
+      const int y = r % kWin, z = r / kWin, ee = ((y | z) & 1) == 0, n = ee ? 8 : kWin;
+      const int o = (int)(sm.rows[r] & 3);
+      const int32_t w[4] = {v[k].x, v[k].y, v[k].z, v[k].w};
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const int xi = 4 * c + i - o;
+        if (xi >= 0 && xi < n) sm.win[Win<T>::at(ee ? 2 * xi + 1 : xi, y, z)] = Fp<T>::with_low_word(w[i]);
+      }
+    }
+  }
+}
+
 template <class T, bool PROG, int PART>
 __global__ void __launch_bounds__(kPredThreads, reconstruct_min_ctas<T, PART>())
 reconstruct_kernel(const int32_t* __restrict__ qc, const T* __restrict__ anchors, Geometry g,
@@ -1359,9 +1411,9 @@ reconstruct_kernel(const int32_t* __restrict__ qc, const T* __restrict__ anchors
   }
   __syncthreads();
   // each code lands in the low word of its window slot (converted when its
-  // point is predicted); every other slot reads as zero.  Two copy groups:
-  // the codes of levels 3..1 (points with all coordinates even), then the
-  // level-0 codes, which arrive while levels 3..1 run.
+  // point is predicted); every other slot reads as zero.  The codes of
+  // levels 3..1 (points with all coordinates even) come first; the level-0
+  // codes follow by one of the three ways below.
   for (int j = tid; j < 729; j += kPredThreads) {
     int x, y, z;
     const int i = even_point<T>(j, x, y, z);
@@ -1374,46 +1426,23 @@ reconstruct_kernel(const int32_t* __restrict__ qc, const T* __restrict__ anchors
   // Level-0 codes by window rows r = z*17 + y: a row with y or z odd holds
   // 17 level-0 points at consecutive slots rows[r] + x, a row with both even
   // its 8 odd-x points at rows[r] + x/2.
-  if (sizeof(T) == 4 && !EDGE && maxlevel >= 0 && (reinterpret_cast<uintptr_t>(qc) & 15) == 0) {
-    // Float interior tile, 16-byte aligned codes: a row's codes lie in at
-    // most five aligned 16-byte chunks (offset o = rows[r] mod 4 plus 17
-    // codes), and chunk s of the tile is chunk s mod 5 of row s / 5.  A
-    // thread's loads are in flight three at a time before their stores; the
-    // words a chunk holds beyond the row (neighbouring rows' codes, or the
-    // code buffer's slack past the last slot) are not stored.  A third of the
-    // fetch instructions of the copies below, but the codes must arrive
-    // before the coarse levels start: faster for float tiles (seven per SM),
-    // slower for double ones (five per SM hide less of that wait).
-    constexpr int kChunks = kWin * kWin * 5, kIt = (kChunks + kPredThreads - 1) / kPredThreads;
-    constexpr int kBatch = (kIt + 1) / 2;
-#pragma unroll
-    for (int k0 = 0; k0 < kIt; k0 += kBatch) {
-      int4 v[kBatch];
-#pragma unroll
-      for (int k = 0; k < kBatch; ++k) {
-        const int s = tid + (k0 + k) * kPredThreads, r = s / 5, c = s - 5 * r;
-        v[k] = make_int4(0, 0, 0, 0);
-        if (k0 + k < kIt && s < kChunks) {
-          const int y = r % kWin, z = r / kWin, n = ((y | z) & 1) ? kWin : 8;
-          const uint64_t first = sm.rows[r];
-          const int o = (int)(first & 3);
-          if (4 * c < o + n) v[k] = __ldg(reinterpret_cast<const int4*>(qc + (first - o)) + c);
-        }
-      }
-#pragma unroll
-      for (int k = 0; k < kBatch; ++k) {
-        const int s = tid + (k0 + k) * kPredThreads, r = s / 5, c = s - 5 * r;
-        if (k0 + k >= kIt || s >= kChunks) continue;
-        const int y = r % kWin, z = r / kWin, ee = ((y | z) & 1) == 0, n = ee ? 8 : kWin;
-        const int o = (int)(sm.rows[r] & 3);
-        const int32_t w[4] = {v[k].x, v[k].y, v[k].z, v[k].w};
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const int xi = 4 * c + i - o;
-          if (xi >= 0 && xi < n) sm.win[Win<T>::at(ee ? 2 * xi + 1 : xi, y, z)] = Fp<T>::with_low_word(w[i]);
-        }
-      }
+  // Interior tiles with 16-byte aligned codes load them in 16-byte chunks
+  // (fetch_level0_vec): a third of the instructions of one copy per code, but
+  // the codes are stored from registers, so the loads must have arrived.
+  // Float tiles (seven per SM) do that before the coarse levels; double
+  // tiles (five per SM, which hide less of that wait) bring the rows into L2
+  // now and load them after the coarse levels (1-3% faster than copies
+  // landing during the coarse levels; loading before them was 3% slower).
+  const bool late = sizeof(T) == 8 && !EDGE && maxlevel >= 0 && (reinterpret_cast<uintptr_t>(qc) & 15) == 0;
+  if (late) {
+    for (int r = tid; r < kWin * kWin; r += kPredThreads) {
+      const int y = r % kWin, z = r / kWin, n = ((y | z) & 1) ? kWin : 8;
+      const int32_t* p = qc + sm.rows[r];
+      prefetch_l2(p);
+      prefetch_l2(p + n - 1);
     }
+  } else if (sizeof(T) == 4 && !EDGE && maxlevel >= 0 && (reinterpret_cast<uintptr_t>(qc) & 15) == 0) {
+    fetch_level0_vec<T>(sm, qc, tid);  // 2.5-9% faster than the copies below
   } else {
     // Each half-warp takes x = 0..15 of one row (the row's slot base is one
     // shared broadcast), then x = 16.
@@ -1454,6 +1483,7 @@ reconstruct_kernel(const int32_t* __restrict__ qc, const T* __restrict__ anchors
   }
   __syncthreads();
   sweep_coarse<T, false, EDGE>(sm.win, nullptr, f.lim, f.last[2], sm.p);
+  if (late) fetch_level0_vec<T>(sm, qc, tid);
   copy_async_wait_group<0>();
   __syncthreads();
   sweep_fine<T, false, EDGE>(sm.win, nullptr, f.lim, f.last[2], sm.p);
