@@ -43,7 +43,7 @@ L2_BYTES = 126 * 1024 * 1024
 # DRAM bytes (read + write) per stage launch from one Nsight Compute capture of
 # this workload (interior + edge launches of a progressive step; see
 # profiles/reconstruct_kernel_progressive_f64_384x384x256.md)
-NCU_TRAFFIC = {"reconstruct": 605.7e6 + 75.9e6}
+NCU_TRAFFIC = {"reconstruct": 612.8e6 + 77.9e6}
 
 
 def measured_peak():
