@@ -100,3 +100,34 @@ def test_predict_and_reconstruct_forced_flags(env, dims, dtype, flag_name):
                 "prism_reconstruct progressive")
         ref2 = O.reconstruct(o_qc, o_anchors, (nz, ny, nx), dtype, eb, md, rv, 0.0, maxlevel, old_np)
         assert np.array_equal(out2.cpu().numpy().view(np.uint8), ref2.view(np.uint8)), f"maxlevel {maxlevel}"
+
+
+@pytest.mark.parametrize("dims", [(70, 45, 33), (48, 32, 64)])
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_reconstruct_from_unaligned_code_buffer(env, dims, dtype):
+    """Interior tiles load their level-0 codes in 16-byte pieces when the code
+    buffer is 16-byte aligned and by 4-byte copies otherwise: a buffer one
+    code off alignment gives the same bytes, fresh and progressive."""
+    torch, P, h = env
+    md, rv = FLAGS["md"]
+    nx, ny, nz = dims
+    data = field(dims, dtype, 11)
+    eb = 1e-3
+    flags8 = (C.c_uint8 * 8)(*md, *rv)
+    codes, anchors = gpu_predict(torch, P, h, data, eb, flags8)
+    shifted = torch.zeros(codes.numel() + 4, dtype=torch.int32, device="cuda")
+    shifted[1:1 + codes.numel()] = codes
+    assert (codes.data_ptr() % 16, shifted[1:].data_ptr() % 16) == (0, 4)
+    l = P.lib()
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    old = torch.from_numpy(field(dims, dtype, 5)).cuda()
+    for prev in (None, old):
+        outs = []
+        for buf in (codes, shifted[1:]):
+            out = torch.empty((nz, ny, nx), dtype=old.dtype, device="cuda")
+            h.check(l.prism_reconstruct(h.ptr, C.c_void_p(buf.data_ptr()), C.c_void_p(anchors.data_ptr()),
+                                        data.itemsize, nx, ny, nz, C.c_double(eb), C.c_double(0.0), flags8, 4,
+                                        None if prev is None else C.c_void_p(prev.data_ptr()),
+                                        C.c_void_p(out.data_ptr()), st), "prism_reconstruct")
+            outs.append(out.cpu().numpy())
+        assert np.array_equal(outs[0].view(np.uint8), outs[1].view(np.uint8))
