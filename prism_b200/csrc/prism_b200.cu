@@ -93,6 +93,7 @@ struct ProgMirror {
 
 struct prism_handle {
   DevBuf qc, planes, status, offs, bsum, part, wins, ranges, anchors, small, dev_in, dev_out, zero_anchors;
+  DevBuf qc_odd;  // the code buffer of a progressive object's odd-numbered steps
   DevBuf sbatch;  // batched strategy searches: cells, inputs and states
   // Pinned host memory mapped into the device: kernels store the results the
   // host reads (sizes, flags, parameters, progressive state) straight into
@@ -114,14 +115,16 @@ struct prism_handle {
   // launch (the two write disjoint tiles)
   cudaStream_t side = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
-  // Progressive steps run their strategy, plan and decode on `dec` so that a
-  // step's decode overlaps the previous step's reconstruction: the decode
-  // needs only the plane buffer, which the previous inverse shuffle (event
-  // planes_free) has consumed.  epoch counts the calls that use the handle's
-  // buffers; a step takes the short wait only when the previous such call
-  // was the previous step of the same object on the same stream.
+  // Progressive steps run their strategy, plan, decode and inverse shuffle on
+  // `dec` so that they overlap the previous step's reconstruction: step k
+  // writes its codes and parameters to slot k mod 2 (qc / qc_odd, params /
+  // params_odd), whose last reader was the reconstruction of step k - 2
+  // (event recon_done[slot]); the plane buffer is only touched on `dec`.
+  // epoch counts the calls that use the handle's buffers; a step takes the
+  // short wait only when the previous such call was the previous step of the
+  // same object on the same stream.
   cudaStream_t dec = nullptr;
-  cudaEvent_t dec_call = nullptr, dec_done = nullptr, planes_free = nullptr;
+  cudaEvent_t dec_call = nullptr, dec_done = nullptr, recon_done[2] = {nullptr, nullptr};
   uint64_t epoch = 0, chain_epoch = 0;
   const void* chain_prog = nullptr;
   cudaStream_t chain_stream = nullptr;
@@ -688,7 +691,7 @@ void prism_destroy(prism_handle* h) {
   if (h->fork) cudaEventDestroy(h->fork);
   if (h->join) cudaEventDestroy(h->join);
   if (h->dec) cudaStreamDestroy(h->dec);
-  for (cudaEvent_t e : {h->dec_call, h->dec_done, h->planes_free})
+  for (cudaEvent_t e : {h->dec_call, h->dec_done, h->recon_done[0], h->recon_done[1]})
     if (e) cudaEventDestroy(e);
   if (h->host) cudaFreeHost(h->host);
   if (h->prog_host) cudaFreeHost(h->prog_host);
@@ -937,11 +940,14 @@ static int progressive_step_t(prism_prog* p, double target, const T* prev, T* va
     CK(cudaStreamCreateWithFlags(&h->dec, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&h->dec_call, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&h->dec_done, cudaEventDisableTiming));
-    CK(cudaEventCreateWithFlags(&h->planes_free, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&h->recon_done[0], cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&h->recon_done[1], cudaEventDisableTiming));
   }
   cudaStream_t dst = h->dec;
+  const int slot = (int)(p->steps & 1);
   if (chained) {
-    CK(cudaStreamWaitEvent(dst, h->planes_free, 0));
+    // the slot's codes and parameters were last read two steps back
+    CK(cudaStreamWaitEvent(dst, h->recon_done[slot], 0));
   } else {
     CK(cudaEventRecord(h->dec_call, st));
     CK(cudaStreamWaitEvent(dst, h->dec_call, 0));
@@ -960,9 +966,12 @@ static int progressive_step_t(prism_prog* p, double target, const T* prev, T* va
   const double* range = reinterpret_cast<const double*>(tr + 8);
   bool first = p->steps == 0;
   StrategyState* ds = p->d_state;
-  // parameters alternate between two slots, so that the next step's plan can
-  // run while this step's reconstruction reads its own
-  PredParams<T>* params = reinterpret_cast<PredParams<T>*>((p->steps & 1) ? s->params_odd : s->params);
+  // parameters and codes alternate between two slots, so that the next
+  // step's plan and inverse shuffle can run while this step's reconstruction
+  // reads its own
+  PredParams<T>* params = reinterpret_cast<PredParams<T>*>(slot ? s->params_odd : s->params);
+  if (slot) CKA(h->qc_odd.ensure(qc_len(g) * sizeof(int32_t)));
+  int32_t* codes = slot ? h->qc_odd.as<int32_t>() : h->qc.as<int32_t>();
   // ---- on the decode stream: strategy, plan, chunk offsets, decode, state
   if (first) {  // no planes loaded, all levels, no errors
     prog_init_kernel<<<1, 32, 0, dst>>>(ds, p->d_err);
@@ -998,21 +1007,21 @@ static int progressive_step_t(prism_prog* p, double target, const T* prev, T* va
   // the state after the step (plane ranges, errors, bytes loaded) for the host
   prog_publish_kernel<<<1, 32, 0, dst>>>(ds, p->d_err, csbp, p->mirror_dev);
   h->launches += 1;
-  CK(cudaEventRecord(h->dec_done, dst));
-  // ---- on the caller's stream: inverse shuffle, reconstruction
-  CK(cudaStreamWaitEvent(st, h->dec_done, 0));
-  rc = launch_inverse(h, h->planes.as<uint8_t>(), g, 1 /*NB*/, ds->begin, ds->end, h->qc.as<int32_t>(), st);
+  rc = launch_inverse(h, h->planes.as<uint8_t>(), g, 1 /*NB*/, ds->begin, ds->end, codes, dst);
   if (rc) return rc;
-  CK(cudaEventRecord(h->planes_free, st));
+  CK(cudaEventRecord(h->dec_done, dst));
+  // ---- on the caller's stream: reconstruction
+  CK(cudaStreamWaitEvent(st, h->dec_done, 0));
   prof_begin(h, kStReconstruct, st);
   if (first) {
-    rc = launch_reconstruct<T, false>(h, h->qc.as<int32_t>(), reinterpret_cast<const T*>(tr + 1040), g, params,
-                                      nullptr, values, st);
+    rc = launch_reconstruct<T, false>(h, codes, reinterpret_cast<const T*>(tr + 1040), g, params, nullptr, values,
+                                      st);
   } else {
-    rc = launch_reconstruct<T, true>(h, h->qc.as<int32_t>(), h->zero_anchors.as<T>(), g, params, prev, values, st);
+    rc = launch_reconstruct<T, true>(h, codes, h->zero_anchors.as<T>(), g, params, prev, values, st);
   }
   if (rc) return rc;
   prof_end(h, kStReconstruct, st);
+  CK(cudaEventRecord(h->recon_done[slot], st));
   CK(cudaGetLastError());
   CK(cudaEventRecord(p->done, st));
   p->pending = true;
