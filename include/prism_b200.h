@@ -110,7 +110,10 @@ int prism_decompress_host(prism_handle* h, const void* h_container, uint64_t siz
  * values in d_values in place (the first step overwrites them).  A step is
  * enqueued on `stream` and returns without waiting (the plane state stays in
  * device memory); prism_progressive_state waits for the last step and
- * returns PRISM_ERR_CORRUPT if any step met a corrupt chunk. */
+ * returns PRISM_ERR_CORRUPT if any step met a corrupt chunk.  From an
+ * object's second step on, the handle holds a second code buffer
+ * (prism_code_buffer_len entries) so that a step's decode and inverse shuffle
+ * can run beside the previous step's reconstruction. */
 int prism_progressive_open(prism_handle* h, const void* d_container, uint64_t size, int dtype_size,
                            uint32_t nx, uint32_t ny, uint32_t nz, int mode, double bound,
                            prism_prog** out);
