@@ -55,7 +55,10 @@ enum prism_status {
 typedef struct prism_handle prism_handle;
 typedef struct prism_prog prism_prog;
 
-/* Handle owning the device workspace (grown on demand, reused across calls). */
+/* Handle owning the device workspace (grown on demand, reused across calls).
+ * The calls on one handle share that workspace: enqueue them on one stream,
+ * or order the streams they use (one handle per concurrent stream, as the
+ * server's workers do). */
 int prism_create(prism_handle** out);
 void prism_destroy(prism_handle* h);
 /* Human-readable description of the last failure on this handle. */
