@@ -278,25 +278,65 @@ __global__ void params_kernel(int mode, double bound, const double* __restrict__
 // Global min / max (compressor.cu:230-302): per-block partials, then one block.
 constexpr int kExtThreads = 512;
 
+// 16-byte vectors of values for the extrema scan
+template <class T> struct Vec16;
+template <> struct Vec16<double> {
+  using type = double2;
+  static __device__ __forceinline__ void fold(const double2& v, double& mn, double& mx) {
+    mn = v.x < mn ? v.x : mn;
+    mx = v.x > mx ? v.x : mx;
+    mn = v.y < mn ? v.y : mn;
+    mx = v.y > mx ? v.y : mx;
+  }
+};
+template <> struct Vec16<float> {
+  using type = float4;
+  static __device__ __forceinline__ void fold(const float4& v, float& mn, float& mx) {
+    mn = v.x < mn ? v.x : mn;
+    mx = v.x > mx ? v.x : mx;
+    mn = v.y < mn ? v.y : mn;
+    mx = v.y > mx ? v.y : mx;
+    mn = v.z < mn ? v.z : mn;
+    mx = v.z > mx ? v.z : mx;
+    mn = v.w < mn ? v.w : mn;
+    mx = v.w > mx ? v.w : mx;
+  }
+};
+
+// The folds start from in[0] and keep the running value unless the new one
+// compares below (above) it, so a NaN is skipped unless it is in[0], and the
+// result does not depend on the order in which values are folded.
 template <class T>
 __global__ void __launch_bounds__(kExtThreads)
 extrema_kernel(const T* __restrict__ in, uint64_t n, T* __restrict__ part) {
+  using V = typename Vec16<T>::type;
+  constexpr uint64_t W = 16 / sizeof(T);
   __shared__ T smin[kExtThreads], smax[kExtThreads];
   T mn = in[0], mx = in[0];
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  for (; i + 3 * stride < n; i += 4 * stride) {  // four independent loads in flight
-    T v[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) v[k] = __ldg(in + i + k * stride);
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      mn = v[k] < mn ? v[k] : mn;
-      mx = v[k] > mx ? v[k] : mx;
-    }
+  const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  // values before the first 16-byte boundary, the 16-byte vectors (four
+  // independent loads in flight), the values after the last whole vector
+  uint64_t head = ((16 - (reinterpret_cast<uintptr_t>(in) & 15)) & 15) / sizeof(T);
+  head = head < n ? head : n;
+  const uint64_t nv = (n - head) / W, tail = head + nv * W;
+  if (tid < head) {
+    const T v = __ldg(in + tid);
+    mn = v < mn ? v : mn;
+    mx = v > mx ? v : mx;
   }
-  for (; i < n; i += stride) {
-    T v = __ldg(in + i);
+  const V* vin = reinterpret_cast<const V*>(in + head);
+  uint64_t i = tid;
+  for (; i + 3 * stride < nv; i += 4 * stride) {
+    V v[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) v[k] = __ldg(vin + i + k * stride);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) Vec16<T>::fold(v[k], mn, mx);
+  }
+  for (; i < nv; i += stride) Vec16<T>::fold(__ldg(vin + i), mn, mx);
+  if (tail + tid < n) {
+    const T v = __ldg(in + tail + tid);
     mn = v < mn ? v : mn;
     mx = v > mx ? v : mx;
   }

@@ -94,6 +94,7 @@ struct ProgMirror {
 struct prism_handle {
   DevBuf qc, planes, status, offs, bsum, part, wins, ranges, anchors, small, dev_in, dev_out, zero_anchors;
   DevBuf qc_odd;  // the code buffer of a progressive object's odd-numbered steps
+  DevBuf ext;     // per-CTA partials of the extrema scan
   DevBuf sbatch;  // batched strategy searches: cells, inputs and states
   // Pinned host memory mapped into the device: kernels store the results the
   // host reads (sizes, flags, parameters, progressive state) straight into
@@ -354,13 +355,15 @@ static const PredParams<T>* params_ptr(prism_handle* h) {
 
 // ---- stage launchers ----
 
+// per_sm: extrema CTAs per SM (four fill an SM; two, with 16-byte loads, still
+// keep the copy bandwidth and leave room for the auto-tune beside them)
 template <class T>
-static int launch_extrema(prism_handle* h, const T* in, uint64_t n, cudaStream_t st) {
-  int blocks = (int)std::min<uint64_t>((n + kExtThreads - 1) / kExtThreads, (uint64_t)h->sm_count * 4);
-  CKA(h->part.ensure(sizeof(T) * 2 * blocks));
+static int launch_extrema(prism_handle* h, const T* in, uint64_t n, cudaStream_t st, int per_sm = 4) {
+  int blocks = (int)std::min<uint64_t>((n + kExtThreads - 1) / kExtThreads, (uint64_t)h->sm_count * per_sm);
+  CKA(h->ext.ensure(sizeof(T) * 2 * blocks));
   prof_begin(h, kStExtrema, st);
-  extrema_kernel<T><<<blocks, kExtThreads, 0, st>>>(in, n, h->part.as<T>());
-  extrema_final_kernel<T><<<1, 32, 0, st>>>(h->part.as<T>(), blocks, &small(h)->range, small(h)->minmax);
+  extrema_kernel<T><<<blocks, kExtThreads, 0, st>>>(in, n, h->ext.as<T>());
+  extrema_final_kernel<T><<<1, 32, 0, st>>>(h->ext.as<T>(), blocks, &small(h)->range, small(h)->minmax);
   prof_end(h, kStExtrema, st);
   h->launches += 2;
   CK(cudaGetLastError());
@@ -369,49 +372,61 @@ static int launch_extrema(prism_handle* h, const T* in, uint64_t n, cudaStream_t
 
 __global__ void set_double_kernel(double* p, double v) { *p = v; }
 
+static double alpha_of(double r);
+
+// the auto-tune's error sums over the sample windows (no dependence on the
+// error bound, so it can run beside the extrema scan)
 template <class T>
-static int launch_autotune_params(prism_handle* h, const T* in, const Geometry& g, int mode, double bound,
-                                  double rel_for_alpha, const uint8_t* force_flags_dev, cudaStream_t st) {
+static int launch_autotune(prism_handle* h, const T* in, const Geometry& g, cudaStream_t st) {
   std::vector<SampleWindow> wins = sample_grid(g.nx, g.ny, g.nz);
-  int nwin = (int)wins.size();
-  double alpha = 1.0;
-  {
-    const double a1 = 2.0, a2 = 1.75, a3 = 1.5, a4 = 1.25, a5 = 1;
-    const double e1 = 1e-1, e2 = 1e-2, e3 = 1e-3, e4 = 1e-4, e5 = 1e-5;
-    double r = rel_for_alpha;  // InterpolationPredictor.cu:2248-2271
-    if (r >= e1) alpha = a1;
-    else if (r >= e2) alpha = a2 + (a1 - a2) * (r - e2) / (e1 - e2);
-    else if (r >= e3) alpha = a3 + (a2 - a3) * (r - e3) / (e2 - e3);
-    else if (r >= e4) alpha = a4 + (a3 - a4) * (r - e4) / (e3 - e4);
-    else if (r >= e5) alpha = a5 + (a4 - a5) * (r - e5) / (e4 - e5);
-    else alpha = a5;
+  const int nwin = (int)wins.size();
+  CKA(h->part.ensure(sizeof(T) * 15 * std::max(nwin, 1) + 64));
+  if (nwin > 0) {
+    if (h->wins_dims[0] != g.nx || h->wins_dims[1] != g.ny || h->wins_dims[2] != g.nz) {
+      CKA(h->wins.ensure(sizeof(SampleWindow) * nwin));
+      CK(cudaMemcpyAsync(h->wins.p, wins.data(), sizeof(SampleWindow) * nwin, cudaMemcpyHostToDevice, st));
+      h->wins_dims[0] = g.nx;
+      h->wins_dims[1] = g.ny;
+      h->wins_dims[2] = g.nz;
+    }
+    prof_begin(h, kStAutotune, st);
+    autotune_kernel<T><<<dim3(nwin, 6), kAttThreads, 0, st>>>(in, g, h->wins.as<SampleWindow>(), h->part.as<T>());
+    prof_end(h, kStAutotune, st);
+    h->launches += 1;
   }
+  CK(cudaGetLastError());
+  return PRISM_OK;
+}
+
+// the decisions and per-level parameters from the sums (or forced flags) and
+// the range
+template <class T>
+static int launch_params(prism_handle* h, const Geometry& g, int mode, double bound, double rel_for_alpha,
+                         const uint8_t* force_flags_dev, cudaStream_t st) {
+  const double alpha = alpha_of(rel_for_alpha);  // InterpolationPredictor.cu:2248-2271
   Small* s = small(h);
   if (!force_flags_dev) {
-    CKA(h->part.ensure(sizeof(T) * 15 * std::max(nwin, 1) + 64));
-    if (nwin > 0) {
-      if (h->wins_dims[0] != g.nx || h->wins_dims[1] != g.ny || h->wins_dims[2] != g.nz) {
-        CKA(h->wins.ensure(sizeof(SampleWindow) * nwin));
-        CK(cudaMemcpyAsync(h->wins.p, wins.data(), sizeof(SampleWindow) * nwin, cudaMemcpyHostToDevice, st));
-        h->wins_dims[0] = g.nx;
-        h->wins_dims[1] = g.ny;
-        h->wins_dims[2] = g.nz;
-      }
-      prof_begin(h, kStAutotune, st);
-      autotune_kernel<T><<<dim3(nwin, 6), kAttThreads, 0, st>>>(in, g, h->wins.as<SampleWindow>(), h->part.as<T>());
-      prof_end(h, kStAutotune, st);
-      h->launches += 1;
-    }
+    const int nwin = (int)sample_grid(g.nx, g.ny, g.nz).size();
     params_kernel<T><<<1, 32, 0, st>>>(mode, bound, &s->range, alpha, h->part.as<T>(), nwin, nullptr, 4,
                                        reinterpret_cast<PredParams<T>*>(s->params),
                                        reinterpret_cast<T*>(s->errors), &s->eb);
-    h->launches += 1;
   } else {
     params_kernel<T><<<1, 32, 0, st>>>(mode, bound, &s->range, alpha, nullptr, 0, force_flags_dev, 4,
                                        reinterpret_cast<PredParams<T>*>(s->params), nullptr, &s->eb);
   }
+  h->launches += 1;
   CK(cudaGetLastError());
   return PRISM_OK;
+}
+
+template <class T>
+static int launch_autotune_params(prism_handle* h, const T* in, const Geometry& g, int mode, double bound,
+                                  double rel_for_alpha, const uint8_t* force_flags_dev, cudaStream_t st) {
+  if (!force_flags_dev) {
+    const int rc = launch_autotune<T>(h, in, g, st);
+    if (rc) return rc;
+  }
+  return launch_params<T>(h, g, mode, bound, rel_for_alpha, force_flags_dev, st);
 }
 
 static double alpha_of(double r) {
@@ -597,12 +612,19 @@ static int compress_t(prism_handle* h, const T* in, const Geometry& g, int mode,
   if (cap < need) return fail(h, PRISM_ERR_ARG, "output capacity below prism_max_container_size");
   Small* s = small(h);
   if (mode == 1) {
-    rc = launch_extrema<T>(h, in, g.n, st);
-    if (rc) return rc;
+    // the extrema scan (two CTAs per SM) and the auto-tune side by side
+    int rc_ext = PRISM_OK, rc_att = PRISM_OK;
+    CK(fork_join(
+        h, st, true, true, [&](cudaStream_t x) { rc_ext = launch_extrema<T>(h, in, g.n, x, 2); },
+        [&](cudaStream_t x) { rc_att = launch_autotune<T>(h, in, g, x); }));
+    if (rc_ext) return rc_ext;
+    if (rc_att) return rc_att;
   } else {
     set_double_kernel<<<1, 1, 0, st>>>(&s->range, 1.0);
+    rc = launch_autotune<T>(h, in, g, st);
+    if (rc) return rc;
   }
-  rc = launch_autotune_params<T>(h, in, g, mode, bound, mode == 1 ? bound : 0.0, nullptr, st);
+  rc = launch_params<T>(h, g, mode, bound, mode == 1 ? bound : 0.0, nullptr, st);
   if (rc) return rc;
   rc = zero_code_padding(h, g, st);
   if (rc) return rc;
@@ -679,7 +701,7 @@ void prism_destroy(prism_handle* h) {
   if (!h) return;
   DevBuf* bufs[] = {&h->qc, &h->planes, &h->status, &h->offs, &h->bsum, &h->part, &h->wins, &h->ranges,
                     &h->anchors, &h->small, &h->dev_in, &h->dev_out, &h->zero_anchors, &h->prog_slots,
-                    &h->sbatch};
+                    &h->sbatch, &h->qc_odd, &h->ext};
   for (DevBuf* b : bufs) b->release();
   for (DevBuf& b : h->prog_offs) b.release();
   for (int i = 0; i < kStCount; ++i)
